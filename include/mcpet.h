@@ -1,0 +1,275 @@
+/* mcpet.h -- C ABI of the B200 (sm_100a) photon-transport path of MCGPU-PET.
+ *
+ * The reference has no library API: its transport path is reached through the
+ * command line program (MCGPU-PET.cu:77-840) and, inside it, through the
+ * track_particles kernel contract (MCGPU-PET_kernel.cu:153-187, prototype
+ * MCGPU-PET.h:523-524) fed by read_input / load_voxels / load_material /
+ * init_CUDA_device.  Each entry point below names the reference code it
+ * replaces.  All functions return an mcpet_status and never exit(); the text
+ * of the last error on the calling thread is available from mcpet_last_error.
+ *
+ * Plain C types only.  Host buffers are caller-owned.  Device pointers (the
+ * *_device entry points) are caller-owned CUDA allocations on the scene's
+ * device; work is ordered on the caller's stream (cudaStream_t passed as
+ * void*; NULL = legacy default stream).
+ */
+#ifndef MCPET_H_
+#define MCPET_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCPET_MAX_MATERIALS 15   /* MCGPU-PET.h:96 */
+#define MCPET_MAX_SHELLS 30      /* MCGPU-PET.h:97 */
+#define MCPET_NP_RAYLEIGH 128    /* MCGPU-PET.h:98 */
+#define MCPET_MAX_ENERGY_BINS 25005 /* MCGPU-PET.h:99 (MAX_ENERGYBINS_RAYLEIGH) */
+#define MCPET_PSF_RECORD_BYTES 44 /* packed PSF_element_struct, MCGPU-PET.h:235-247 */
+
+typedef enum {
+  MCPET_OK = 0,
+  MCPET_ERR_ARG = 1,        /* invalid argument or unsupported value */
+  MCPET_ERR_IO = 2,         /* file missing / unreadable / unwritable */
+  MCPET_ERR_FORMAT = 3,     /* malformed input, voxel or material file */
+  MCPET_ERR_CUDA = 4,       /* CUDA runtime error */
+  MCPET_ERR_NOMEM = 5,      /* host or device allocation failed */
+  MCPET_ERR_LIMIT = 6,      /* a size limit of the format was exceeded */
+  MCPET_ERR_DEVICE = 7      /* a device-side guard fired (loop cap, bad index) */
+} mcpet_status;
+
+/* Lane decomposition of the emission process. */
+typedef enum {
+  /* One lane per (emitting voxel, thread) with threads_per_block lanes per
+   * voxel and RANECU stream id voxel*threads_per_block+thread: the lane set
+   * and random streams of the reference launch (MCGPU-PET.cu:457-483,
+   * MCGPU-PET_kernel.cu:251-253).  Histories replay the reference's. */
+  MCPET_LANES_REFERENCE = 0,
+  /* Lanes per voxel proportional to its expected decays (about
+   * histories_per_lane decays each), stream ids = lane index.  Same emission
+   * statistics (sum of independent Poisson processes), balanced work. */
+  MCPET_LANES_BALANCED = 1
+} mcpet_lane_mode;
+
+/* Everything the reference reads from its input file (read_input,
+ * MCGPU-PET.cu:866-1280), in the same units.  acquisition_time_ps is
+ * (unsigned long long)(seconds*1e12+0.5) as at MCGPU-PET.cu:979. */
+typedef struct {
+  /* [SECTION SIMULATION CONFIG v.2016-07-05] */
+  int seed;                       /* 0 in the file = time-based seed (resolved at parse time) */
+  int gpu_id;
+  int threads_per_block;
+  float density_factor;           /* "fact_object" */
+  /* [SECTION SOURCE PET SCAN v.2017-03-14] */
+  unsigned long long acquisition_time_ps;
+  float mean_life;
+  float material_activity[MCPET_MAX_MATERIALS]; /* parsed; unused by the transport (as in the reference) */
+  /* [SECTION PHASE SPACE FILE v.2016-07-05] */
+  char psf_file[250];
+  float detector_center[3];       /* after auto-centring when radius was < 0 */
+  float detector_height;
+  float detector_radius;
+  int psf_size;
+  int tally_type;                 /* 0 both, 1 trues only, 2 scatter only */
+  int tally_psf_sinogram;         /* 0 both, 1 PSF only, 2 sinogram only */
+  int detector_auto_center;       /* 1 when the file gave a negative radius */
+  /* [SECTION DOSE DEPOSITION v.2012-12-12] */
+  int tally_material_dose;        /* 1 YES, 0 NO */
+  int tally_voxel_dose;           /* 1 YES, 0 NO */
+  char dose_file[250];
+  short dose_roi[6];              /* x_min,x_max,y_min,y_max,z_min,z_max (0-based) */
+  /* [SECTION ENERGY PARAMETERS v.2019-04-25] (eV despite the file's label) */
+  float energy_resolution;
+  float energy_window_low;
+  float energy_window_high;
+  /* [SECTION SINOGRAM PARAMETERS v.2019-04-25] */
+  float fov_z;
+  int n_rows, n_crystals, n_angles, n_radial, n_z_slices, image_res, n_energy_bins;
+  int max_ring_difference, span;
+  int n_segments, n_sinograms;    /* derived as at MCGPU-PET.cu:1176-1187 */
+  long long n_bins;               /* n_radial*n_angles*n_sinograms, 64-bit */
+  /* [SECTION VOXELIZED GEOMETRY FILE v.2009-11-30] / [SECTION MATERIAL FILE LIST] */
+  char voxel_file[250];
+  char material_files[MCPET_MAX_MATERIALS][250];
+} mcpet_config;
+
+typedef struct mcpet_scene mcpet_scene;   /* opaque: phantom + tables + device copy */
+
+typedef struct {
+  int nx, ny, nz;
+  float voxel_size[3];
+  float bbox[3];
+  long long n_voxels;
+  long long n_emitting_voxels;
+  double total_activity_bq;
+  int n_energy;                   /* rows of the material tables */
+  float e0, inv_de;               /* first energy (eV), inverse step (1/eV) */
+  int n_materials_used;
+  int n_palette;                  /* distinct (material, density) pairs in the phantom */
+  float density_max[MCPET_MAX_MATERIALS];
+  float density_nominal[MCPET_MAX_MATERIALS];
+  long long n_bins;
+  int n_energy_spectrum;
+} mcpet_scene_info;
+
+typedef struct {
+  int lane_mode;                  /* mcpet_lane_mode */
+  int background_mode;            /* 1 = second photon isotropic (reference's 2-argument CLI, PETA_DEV[0]==0) */
+  int histories_per_lane;         /* balanced mode: expected decays per lane (<=0: automatic) */
+  int block_threads;              /* CUDA threads per block of the transport kernel (<=0: automatic) */
+  int blocks_per_sm;              /* resident blocks per SM for the persistent grid (<=0: automatic) */
+  int collect_counters;           /* 1: also fill mcpet_tallies.counters (slower kernel variant) */
+  int seed_override;              /* != 0: use this RANECU seed instead of the scene's */
+  void* stream;                   /* cudaStream_t; NULL = default stream */
+} mcpet_run_opts;
+
+/* Event counters (when collect_counters=1). */
+typedef struct {
+  unsigned long long woodcock_steps_inside;  /* steps that landed inside the phantom */
+  unsigned long long table_refreshes;        /* (material, energy) table reloads */
+  unsigned long long majorant_refreshes;     /* energy changes (Woodcock table reads) */
+  unsigned long long tally_increments;       /* int32 tally increments (sinogram+image+spectrum) */
+  unsigned long long photons;                /* photon histories started */
+  unsigned long long compton, rayleigh, photoelectric;
+  unsigned long long lanes;
+  unsigned long long guard_trips;            /* loop caps / index guards that fired */
+} mcpet_counters;
+
+/* Output tallies (int32 as in the reference, MCGPU-PET.cu:279-298).
+ * Any pointer may be NULL to skip that download / tally. */
+typedef struct {
+  int32_t* trues;                 /* [n_bins] sinogram of true coincidences */
+  int32_t* scatter;               /* [n_bins] sinogram of scatter coincidences */
+  int32_t* image_trues;           /* [n_voxels] emission voxel of detected trues */
+  int32_t* image_scatter;         /* [n_voxels] emission voxel of detected scatter */
+  int32_t* spectrum;              /* [n_energy_spectrum] 1 keV bins, before the window */
+  void* psf;                      /* psf_capacity packed 44-byte records */
+  long long psf_capacity;         /* elements; the reference's PSF_size */
+  int32_t* psf_count;             /* the reference's index_PSF after the run */
+  unsigned long long* total_histories;  /* photons (2 per decay), MCGPU-PET_kernel.cu:282 */
+  mcpet_counters* counters;
+  double* transport_ms;           /* device time of the transport kernel(s) */
+} mcpet_tallies;
+
+/* ---- configuration and scene (host) ---------------------------------- */
+
+/* Parse an input file.  Replaces read_input (MCGPU-PET.cu:866-1280) incl. the
+ * NSEG/NSINOS/NBINS derivation (:1176-1189).  Relative paths inside the file
+ * are kept as written (resolved against the working directory on load, as the
+ * reference does). */
+mcpet_status mcpet_config_read(const char* in_path, mcpet_config* cfg);
+
+/* Parse the input file, read the .vox phantom and material tables and build
+ * the interpolation tables.  Replaces read_input + load_voxels
+ * (MCGPU-PET.cu:1381-1533) + load_material (:1565-1831) + the detector
+ * auto-centring in main (:316-322) + the 511 keV coverage check (:344-351). */
+mcpet_status mcpet_scene_load(const char* in_path, mcpet_scene** out);
+
+/* Same as mcpet_scene_load but from in-memory voxel arrays (x fastest, then
+ * y, then z; material 1-based as in the .vox file; density before the
+ * density_factor scale).  Material tables are read from cfg->material_files. */
+mcpet_status mcpet_scene_from_arrays(const mcpet_config* cfg, int nx, int ny, int nz,
+                                     const float voxel_size_cm[3], const int32_t* material,
+                                     const float* density, const float* activity,
+                                     mcpet_scene** out);
+
+/* Replace the per-voxel activity (Bq) of an existing scene, same length as the
+ * phantom.  The device copy is refreshed lazily on the next run. */
+mcpet_status mcpet_scene_set_activity(mcpet_scene* scene, const float* activity);
+
+mcpet_status mcpet_scene_get_config(const mcpet_scene* scene, mcpet_config* cfg);
+mcpet_status mcpet_scene_get_info(const mcpet_scene* scene, mcpet_scene_info* info);
+
+/* Export the host tables built by the loader, in the reference layout
+ * (MCGPU-PET.h:206-360): woodcock float2[n_e] (x=a, y=b), mfp_a/mfp_b
+ * float3[n_e*15], voxels float3[n_voxels] (material+0.0001, density,
+ * activity).  Compton/Rayleigh arrays as the struct members.  Any pointer may
+ * be NULL.  Used by the parity tests against the reference loaders. */
+mcpet_status mcpet_scene_export_tables(const mcpet_scene* scene, float* woodcock, float* mfp_a,
+                                       float* mfp_b, float* voxels, float* fco, float* uico,
+                                       float* fj0, int32_t* noscco, float* xco, float* pco,
+                                       float* aco, float* bco, float* pmax, uint8_t* itlco,
+                                       uint8_t* ituco);
+
+void mcpet_scene_free(mcpet_scene* scene);
+
+/* ---- transport on the GPU ---------------------------------------------- */
+
+/* Select the CUDA device (<0: the scene's gpu_id, clamped to the available
+ * devices) and upload the scene (palette-compressed voxels, tables, lane
+ * plan).  Replaces init_CUDA_device (MCGPU-PET.cu:1842-2146).  Called
+ * implicitly by the run functions. */
+mcpet_status mcpet_scene_to_device(mcpet_scene* scene, int device);
+
+/* End-to-end run with HOST output buffers: zero the device tallies, run the
+ * transport, download the tallies into *out.  Replaces the launch and
+ * downloads of main (MCGPU-PET.cu:408-535).  Blocking. */
+mcpet_status mcpet_run(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_tallies* out);
+
+/* Run with DEVICE output buffers (caller-allocated on the scene's device,
+ * zeroed by this call), ordered on opts->stream, no host synchronisation
+ * except when counters or transport_ms are requested.  psf_count,
+ * total_histories and counters must then be device pointers too. */
+mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
+                              mcpet_tallies* device_out);
+
+/* Device-side guard status of the last run on this scene (blocking read). */
+mcpet_status mcpet_last_run_guard(mcpet_scene* scene, unsigned long long* trips);
+
+/* ---- outputs ----------------------------------------------------------- */
+
+/* Write the reference's output files into out_dir (NULL = current
+ * directory): sinogram_{Trues,Scatter}.raw.gz and image_{Trues,Scatter}.raw.gz
+ * (or sinogram_BG_*.raw.gz / BG_image_*.raw.gz in background mode) when the
+ * sinogram is tallied, Energy_Sinogram_Spectrum.dat always, and the PSF text
+ * and .raw files when the PSF is tallied.  Replaces MCGPU-PET.cu:503-616 and
+ * report_PSF (:3193-3322). */
+mcpet_status mcpet_write_outputs(const mcpet_scene* scene, const mcpet_tallies* host,
+                                 const char* out_dir, int background_mode, double elapsed_s);
+
+/* ---- verification hooks (the reference's device functions, one call per
+ * entry; used by the parity tests against the reference build) ---------- */
+
+/* RANECU lane streams: seed of lane stream id s is the reference init_PRNG
+ * jump (s+1)*555555*256 draws ahead (MCGPU-PET_kernel.cu:925-978), computed on
+ * the GPU; then ndraw float draws and ndraw double draws (ranecu,
+ * ranecu_double :1045-1083) from the same start.  seeds_out[2n]. */
+mcpet_status mcpet_probe_rng(int n, int seed_input, const int64_t* stream_ids, int ndraw,
+                             int32_t* seeds_out, float* draws, double* ddraws);
+
+/* Detector model on a fixed event list (tally_Sinogram,
+ * MCGPU-PET_kernel.cu:1624-1836) on the GPU with the scene's detector and
+ * sinogram geometry.  Per event: out[6*i+0]=bin or -1, +1 class (1 true, 2
+ * scatter, 0 none), +2/+3 spectrum bins of the two photons or -1, +4/+5
+ * seed after the call.  Positions/directions float3, states signed char. */
+mcpet_status mcpet_probe_detector(const mcpet_scene* scene, int n, const float* e2,
+                                  const float* e1, const float* pos2, const float* pos1,
+                                  const float* dir2, const float* dir1, const int8_t* st2,
+                                  const int8_t* st1, const int32_t* seeds, int32_t* out);
+
+/* Compton (GCOa :1335-1563) and Rayleigh (GRAa :1231-1296) sampling on the GPU
+ * with the scene's tables.  Material 0-based. */
+mcpet_status mcpet_probe_compton(const mcpet_scene* scene, int n, const float* energy_in,
+                                 const int32_t* mat, const int32_t* seeds_in, float* energy_out,
+                                 double* costh_out, int32_t* seeds_out);
+mcpet_status mcpet_probe_rayleigh(const mcpet_scene* scene, int n, const float* energy_in,
+                                  const int32_t* mat, const float* pmax, const int32_t* seeds_in,
+                                  double* costh_out, int32_t* seeds_out);
+
+/* Photon-pair source (source :666-773) for every voxel of an nx*ny*nz grid:
+ * out[12*v..] = position1, direction1, position2, direction2. */
+mcpet_status mcpet_probe_source(int nx, int ny, int nz, const float inv_voxel_size[3],
+                                int background_mode, const int32_t* seeds_in, float* out,
+                                int32_t* seeds_out);
+
+/* ---- misc --------------------------------------------------------------- */
+
+const char* mcpet_last_error(void);
+const char* mcpet_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCPET_H_ */

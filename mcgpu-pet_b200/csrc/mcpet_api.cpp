@@ -1,0 +1,831 @@
+/* C ABI of the transport path: scene life cycle, device upload, lane plan,
+ * runs and verification probes. */
+#include <cuda_runtime_api.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "mcpet.h"
+#include "mcpet_kernels.h"
+#include "mcpet_scene.h"
+
+namespace mcpet {
+extern thread_local std::string g_error;
+}
+
+using namespace mcpet;
+
+namespace {
+
+#define CUDA_TRY(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t err_ = (call);                                                                  \
+    if (err_ != cudaSuccess)                                                                    \
+      return set_error(err_ == cudaErrorMemoryAllocation ? MCPET_ERR_NOMEM : MCPET_ERR_CUDA,    \
+                       "%s failed: %s", #call, cudaGetErrorString(err_));                      \
+  } while (0)
+
+template <typename T>
+cudaError_t dmalloc(T** p, size_t bytes) {
+  return cudaMalloc((void**)p, bytes);
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+/* (a^e) mod m with exact 64-bit arithmetic. */
+uint32_t powmod(uint64_t a, uint64_t e, uint64_t m) {
+  uint64_t r = 1 % m;
+  a %= m;
+  while (e) {
+    if (e & 1) r = (r * a) % m;
+    a = (a * a) % m;
+    e >>= 1;
+  }
+  return (uint32_t)r;
+}
+
+/* Powers (a^C)^(2^k) mod m for the stream jump, C = 555555*256 draws per
+ * stream (the reference init_PRNG leap, MCGPU-PET_kernel.cu:251-253,925-978). */
+void jump_tables(int32_t* t1, int32_t* t2) {
+  const uint64_t C = (uint64_t)kLeapHistories * kLeapDistance;
+  uint64_t p1 = powmod(40014, C, 2147483563ull), p2 = powmod(40692, C, 2147483399ull);
+  for (int k = 0; k < 32; ++k) {
+    t1[k] = (int32_t)p1;
+    t2[k] = (int32_t)p2;
+    p1 = (p1 * p1) % 2147483563ull;
+    p2 = (p2 * p2) % 2147483399ull;
+  }
+}
+
+int pick_device(int requested) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) return -1;
+  if (requested < 0 || requested >= count) return 0;
+  return requested;
+}
+
+void fill_params(const mcpet_scene* sc, TransportParams& P) {
+  memset(&P, 0, sizeof(P));
+  const mcpet_config& c = sc->cfg;
+  P.nx = sc->nx;
+  P.ny = sc->ny;
+  P.nz = sc->nz;
+  P.inv_vx = sc->inv_voxel_size[0];
+  P.inv_vy = sc->inv_voxel_size[1];
+  P.inv_vz = sc->inv_voxel_size[2];
+  P.bbx = sc->bbox[0];
+  P.bby = sc->bbox[1];
+  P.bbz = sc->bbox[2];
+  P.n_voxels = (long long)sc->mat0.size();
+  P.n_e = sc->n_e;
+  P.e0 = sc->e0;
+  P.ide = sc->ide;
+  P.cx = c.detector_center[0];
+  P.cy = c.detector_center[1];
+  P.cz = c.detector_center[2];
+  P.radius = c.detector_radius;
+  P.height = c.detector_height;
+  P.psf_capacity = c.psf_size;
+  P.tally_psf_sinogram = c.tally_psf_sinogram;
+  P.tally_type = c.tally_type;
+  P.acq_ps = c.acquisition_time_ps;
+  P.inv_mean_life = 1.0 / (double)c.mean_life;
+  P.e_resol = c.energy_resolution;
+  P.e_low = c.energy_window_low;
+  P.e_high = c.energy_window_high;
+  P.fovz = c.fov_z;
+  P.nrows = c.n_rows;
+  P.ncrystals = c.n_crystals;
+  P.nangles = c.n_angles;
+  P.nrad = c.n_radial;
+  P.nzs = c.n_z_slices;
+  P.ne = c.n_energy_bins;
+  P.mrd = c.max_ring_difference;
+  P.span = c.span;
+  P.nsinos = c.n_sinograms;
+  P.nbins = c.n_bins;
+  jump_tables(P.jump1, P.jump2);
+  P.seed = c.seed;
+  int ms = 1;
+  for (int m = 0; m < kMaxMaterials; ++m)
+    if (sc->material_loaded[m] && sc->compton.noscco[m] > ms) ms = sc->compton.noscco[m];
+  P.max_shells = ms;
+  P.spectrum_in_shared = (c.n_energy_bins > 0 && c.n_energy_bins <= kSpectrumSharedMax) ? 1 : 0;
+  P.palette_in_shared = (sc->palette.size() <= 2048) ? (int)sc->palette.size() : 0;
+}
+
+mcpet_status upload_tables(mcpet_scene* sc) {
+  auto& d = sc->dev;
+  if (d.tables_ready) return MCPET_OK;
+  const size_t nv = sc->mat0.size();
+  d.vox16 = sc->palette.size() <= 65536;
+  if (d.vox16) {
+    std::vector<uint16_t> k(nv);
+    for (size_t i = 0; i < nv; ++i) k[i] = (uint16_t)sc->voxel_key[i];
+    CUDA_TRY(dmalloc(&d.vox, nv * 2));
+    CUDA_TRY(cudaMemcpy(d.vox, k.data(), nv * 2, cudaMemcpyHostToDevice));
+  } else {
+    CUDA_TRY(dmalloc(&d.vox, nv * 4));
+    CUDA_TRY(cudaMemcpy(d.vox, sc->voxel_key.data(), nv * 4, cudaMemcpyHostToDevice));
+  }
+  CUDA_TRY(dmalloc(&d.palette, sc->palette.size() * sizeof(PaletteEntry)));
+  CUDA_TRY(cudaMemcpy(d.palette, sc->palette.data(), sc->palette.size() * sizeof(PaletteEntry),
+                      cudaMemcpyHostToDevice));
+  CUDA_TRY(dmalloc(&d.woodcock, sc->woodcock.size() * 4));
+  CUDA_TRY(cudaMemcpy(d.woodcock, sc->woodcock.data(), sc->woodcock.size() * 4, cudaMemcpyHostToDevice));
+  const size_t nrec = (size_t)sc->n_e * kMaxMaterials;
+  std::vector<MfpRecord> rec(nrec);
+  for (size_t i = 0; i < nrec; ++i) {
+    MfpRecord& r = rec[i];
+    r.ax = sc->mfp_a[3 * i + 0];
+    r.bx = sc->mfp_b[3 * i + 0];
+    r.ay = sc->mfp_a[3 * i + 1];
+    r.by = sc->mfp_b[3 * i + 1];
+    r.az = sc->mfp_a[3 * i + 2];
+    r.bz = sc->mfp_b[3 * i + 2];
+    r.pmax_next = (i + kMaxMaterials < nrec) ? sc->pmax[i + kMaxMaterials] : 0.0f;
+    r.pad = 0.f;
+  }
+  CUDA_TRY(dmalloc(&d.mfp, nrec * sizeof(MfpRecord)));
+  CUDA_TRY(cudaMemcpy(d.mfp, rec.data(), nrec * sizeof(MfpRecord), cudaMemcpyHostToDevice));
+  CUDA_TRY(dmalloc(&d.compton, sizeof(ComptonTable)));
+  CUDA_TRY(cudaMemcpy(d.compton, &sc->compton, sizeof(ComptonTable), cudaMemcpyHostToDevice));
+  const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
+  std::vector<float> ray(4 * nr);
+  std::copy(sc->xco.begin(), sc->xco.end(), ray.begin());
+  std::copy(sc->pco.begin(), sc->pco.end(), ray.begin() + nr);
+  std::copy(sc->aco.begin(), sc->aco.end(), ray.begin() + 2 * nr);
+  std::copy(sc->bco.begin(), sc->bco.end(), ray.begin() + 3 * nr);
+  CUDA_TRY(dmalloc(&d.ray, 4 * nr * 4));
+  CUDA_TRY(cudaMemcpy(d.ray, ray.data(), 4 * nr * 4, cudaMemcpyHostToDevice));
+  std::vector<uint8_t> r8(2 * nr);
+  std::copy(sc->itl.begin(), sc->itl.end(), r8.begin());
+  std::copy(sc->itu.begin(), sc->itu.end(), r8.begin() + nr);
+  CUDA_TRY(dmalloc(&d.ray8, 2 * nr));
+  CUDA_TRY(cudaMemcpy(d.ray8, r8.data(), 2 * nr, cudaMemcpyHostToDevice));
+  CUDA_TRY(dmalloc(&d.small, 16 * sizeof(unsigned long long)));
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  d.ev0 = e0;
+  d.ev1 = e1;
+  d.tables_ready = true;
+  return MCPET_OK;
+}
+
+DeviceTables device_tables(const mcpet_scene* sc) {
+  const auto& d = sc->dev;
+  DeviceTables T;
+  memset(&T, 0, sizeof(T));
+  T.vox16 = d.vox16 ? (const uint16_t*)d.vox : nullptr;
+  T.vox32 = d.vox16 ? nullptr : (const uint32_t*)d.vox;
+  T.palette = d.palette;
+  T.n_palette = (int)sc->palette.size();
+  T.woodcock = d.woodcock;
+  T.mfp = d.mfp;
+  T.compton = d.compton;
+  const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
+  T.rayleigh.xco = d.ray;
+  T.rayleigh.pco = d.ray + nr;
+  T.rayleigh.aco = d.ray + 2 * nr;
+  T.rayleigh.bco = d.ray + 3 * nr;
+  T.rayleigh.itl = d.ray8;
+  T.rayleigh.itu = d.ray8 + nr;
+  T.emitters = d.emitters;
+  return T;
+}
+
+/* Lane plan: emitters (voxels with activity > 1e-7 Bq, the reference's
+ * threshold at MCGPU-PET_kernel.cu:232) with their lane counts and RANECU
+ * streams, ordered by decreasing expected decays per lane. */
+mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
+  auto& d = sc->dev;
+  char key[128];
+  snprintf(key, sizeof(key), "%d/%d/%d", mode, tpb, hpl);
+  if (!d.activity_dirty && d.plan_key == key && d.emitters) return MCPET_OK;
+  const size_t nv = sc->activity.size();
+  const double T = (double)sc->cfg.acquisition_time_ps * 1e-12;
+  std::vector<Emitter> em;
+  em.reserve(1024);
+  for (size_t v = 0; v < nv; ++v) {
+    float a = sc->activity[v];
+    if (!(a > 1.0e-7f)) continue;
+    Emitter e;
+    e.voxel = (uint32_t)v;
+    if (mode == MCPET_LANES_REFERENCE) {
+      e.n_lanes = (uint32_t)tpb;
+      e.stream_base = (uint64_t)v * (uint64_t)tpb;
+      e.inv_rate = (tpb / (double)a);
+    } else {
+      double expect = (double)a * T;
+      double L = ceil(expect / (double)hpl);
+      if (L < 1) L = 1;
+      if (L > 1.0e8) L = 1.0e8;
+      e.n_lanes = (uint32_t)L;
+      e.stream_base = 0;
+      e.inv_rate = (double)e.n_lanes / (double)a;
+    }
+    e.first_lane = 0;
+    em.push_back(e);
+  }
+  std::stable_sort(em.begin(), em.end(), [](const Emitter& x, const Emitter& y) { return x.inv_rate < y.inv_rate; });
+  uint64_t lanes = 0;
+  for (auto& e : em) {
+    e.first_lane = lanes;
+    if (mode != MCPET_LANES_REFERENCE) e.stream_base = lanes;
+    lanes += e.n_lanes;
+  }
+  uint64_t max_stream = 0;
+  for (auto& e : em) max_stream = std::max<uint64_t>(max_stream, e.stream_base + e.n_lanes);
+  if (max_stream >= (1ull << 31))
+    return set_error(MCPET_ERR_LIMIT, "lane plan needs %llu RANECU streams (limit 2^31)",
+                     (unsigned long long)max_stream);
+  if (em.size() > d.emitters_cap) {
+    dfree(d.emitters);
+    size_t cap = std::max<size_t>(em.size(), 1);
+    CUDA_TRY(dmalloc(&d.emitters, cap * sizeof(Emitter)));
+    d.emitters_cap = cap;
+  }
+  if (!em.empty()) CUDA_TRY(cudaMemcpy(d.emitters, em.data(), em.size() * sizeof(Emitter), cudaMemcpyHostToDevice));
+  d.n_emitters = (int)em.size();
+  d.n_lanes = lanes;
+  d.plan_key = key;
+  d.activity_dirty = false;
+  return MCPET_OK;
+}
+
+mcpet_status ensure_device(mcpet_scene* sc) {
+  if (sc->dev.device < 0) return mcpet_scene_to_device(sc, -1);
+  CUDA_TRY(cudaSetDevice(sc->dev.device));
+  return MCPET_OK;
+}
+
+int auto_hpl(const mcpet_scene* sc) {
+  double T = (double)sc->cfg.acquisition_time_ps * 1e-12, D = 0;
+  for (float a : sc->activity)
+    if (a > 1.0e-7f) D += (double)a * T;
+  double threads = (double)std::max(sc->dev.sm_count, 1) * 2048.0;
+  double h = D / (threads * 16.0);
+  if (h < 1) h = 1;
+  if (h > 4096) h = 4096;
+  return (int)h;
+}
+
+/* Enqueue one transport run writing into the device tallies O. */
+mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTallies O, cudaStream_t st,
+                         double* ms_out) {
+  mcpet_status s = ensure_device(sc);
+  if (s != MCPET_OK) return s;
+  s = upload_tables(sc);
+  if (s != MCPET_OK) return s;
+  mcpet_run_opts def;
+  memset(&def, 0, sizeof(def));
+  const mcpet_run_opts& o = opts ? *opts : def;
+  int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
+  int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
+  s = build_lanes(sc, o.lane_mode, tpb, hpl);
+  if (s != MCPET_OK) return s;
+
+  TransportParams P;
+  fill_params(sc, P);
+  if (o.seed_override != 0) P.seed = o.seed_override;
+  if (P.seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", P.seed);
+  P.background_mode = o.background_mode ? 1 : 0;
+  P.n_lanes = sc->dev.n_lanes;
+  P.n_emitters = sc->dev.n_emitters;
+  if (!O.psf) P.psf_capacity = 0;
+
+  const bool sino = sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 2;
+  if (sino && (!O.trues || !O.scatter || !O.image_trues || !O.image_scatter || !O.spectrum))
+    return set_error(MCPET_ERR_ARG, "sinogram tally requested but a sinogram/image/spectrum buffer is missing");
+  if (!O.histories || !O.psf_count) return set_error(MCPET_ERR_ARG, "histories and psf_count are required");
+  if (!P.spectrum_in_shared && !O.spectrum && sino) return set_error(MCPET_ERR_ARG, "spectrum buffer required");
+
+  auto& d = sc->dev;
+  unsigned long long* small = d.small;
+  O.guard = small + 0;
+  O.lane_cursor = small + 1;
+  CUDA_TRY(cudaMemsetAsync(small, 0, 2 * sizeof(unsigned long long), st));
+  const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
+  if (O.trues) CUDA_TRY(cudaMemsetAsync(O.trues, 0, nb, st));
+  if (O.scatter) CUDA_TRY(cudaMemsetAsync(O.scatter, 0, nb, st));
+  if (O.image_trues) CUDA_TRY(cudaMemsetAsync(O.image_trues, 0, nv, st));
+  if (O.image_scatter) CUDA_TRY(cudaMemsetAsync(O.image_scatter, 0, nv, st));
+  if (O.spectrum) CUDA_TRY(cudaMemsetAsync(O.spectrum, 0, (size_t)sc->cfg.n_energy_bins * 4, st));
+  CUDA_TRY(cudaMemsetAsync(O.psf_count, 0, 4, st));
+  CUDA_TRY(cudaMemsetAsync(O.histories, 0, 8, st));
+  if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
+  if (!sino) {
+    /* the kernel only touches the spectrum when the sinogram is tallied */
+    P.spectrum_in_shared = 0;
+  }
+
+  const bool counters = o.collect_counters && O.counters;
+  int block = o.block_threads > 0 ? o.block_threads : transport_block_threads();
+  if (block > transport_block_threads()) block = transport_block_threads();
+  block = (block / 32) * 32;
+  if (block < 32) block = 32;
+  size_t smem = transport_dynamic_smem(P, block);
+  int bps = 0;
+  CUDA_TRY(transport_occupancy(counters, block, smem, &bps));
+  if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
+  if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
+  int grid = d.sm_count * bps;
+  if (P.n_lanes == 0) grid = 1;
+  if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
+  CUDA_TRY(launch_transport(P, device_tables(sc), O, counters, grid, block, smem, st));
+  if (ms_out) {
+    CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
+    CUDA_TRY(cudaEventSynchronize((cudaEvent_t)d.ev1));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, (cudaEvent_t)d.ev0, (cudaEvent_t)d.ev1));
+    *ms_out = ms;
+  }
+  return MCPET_OK;
+}
+
+mcpet_status ensure_run_buffers(mcpet_scene* sc, bool want_psf) {
+  auto& d = sc->dev;
+  long long nb = sc->cfg.n_bins, nv = (long long)sc->mat0.size();
+  int ne = sc->cfg.n_energy_bins;
+  if (d.nbins_alloc != nb) {
+    dfree(d.trues);
+    dfree(d.scatter);
+    CUDA_TRY(dmalloc(&d.trues, (size_t)nb * 4));
+    CUDA_TRY(dmalloc(&d.scatter, (size_t)nb * 4));
+    d.nbins_alloc = nb;
+  }
+  if (d.nvox_alloc != nv) {
+    dfree(d.img_t);
+    dfree(d.img_s);
+    CUDA_TRY(dmalloc(&d.img_t, (size_t)nv * 4));
+    CUDA_TRY(dmalloc(&d.img_s, (size_t)nv * 4));
+    d.nvox_alloc = nv;
+  }
+  if (d.ne_alloc != ne) {
+    dfree(d.spectrum);
+    CUDA_TRY(dmalloc(&d.spectrum, (size_t)std::max(ne, 1) * 4));
+    d.ne_alloc = ne;
+  }
+  long long cap = want_psf ? (long long)std::max(sc->cfg.psf_size, 0) : 0;
+  if (cap != d.psf_cap) {
+    dfree(d.psf);
+    if (cap > 0) CUDA_TRY(dmalloc(&d.psf, (size_t)cap * 44));
+    d.psf_cap = cap;
+  }
+  return MCPET_OK;
+}
+
+}  // namespace
+
+mcpet_scene::~mcpet_scene() {
+  if (dev.device >= 0) {
+    cudaSetDevice(dev.device);
+    dfree(dev.vox);
+    dfree(dev.palette);
+    dfree(dev.woodcock);
+    dfree(dev.mfp);
+    dfree(dev.compton);
+    dfree(dev.ray);
+    dfree(dev.ray8);
+    dfree(dev.emitters);
+    dfree(dev.trues);
+    dfree(dev.scatter);
+    dfree(dev.img_t);
+    dfree(dev.img_s);
+    dfree(dev.spectrum);
+    dfree(dev.psf);
+    dfree(dev.small);
+    if (dev.ev0) cudaEventDestroy((cudaEvent_t)dev.ev0);
+    if (dev.ev1) cudaEventDestroy((cudaEvent_t)dev.ev1);
+  }
+}
+
+extern "C" {
+
+const char* mcpet_last_error(void) { return mcpet::g_error.c_str(); }
+const char* mcpet_version(void) { return "mcpet-b200 0.1 (sm_100a)"; }
+
+mcpet_status mcpet_config_read(const char* in_path, mcpet_config* cfg) { return parse_input(in_path, cfg); }
+
+static mcpet_status load_common(mcpet_scene* sc) {
+  mcpet_status s = load_materials(sc);
+  if (s != MCPET_OK) return s;
+  return finalize_scene(sc);
+}
+
+mcpet_status mcpet_scene_load(const char* in_path, mcpet_scene** out) {
+  if (!out) return set_error(MCPET_ERR_ARG, "null output");
+  *out = nullptr;
+  mcpet_scene* sc = new (std::nothrow) mcpet_scene();
+  if (!sc) return set_error(MCPET_ERR_NOMEM, "out of host memory");
+  mcpet_status s = parse_input(in_path, &sc->cfg);
+  if (s == MCPET_OK) s = load_phantom_file(sc->cfg.voxel_file, sc->cfg.density_factor, sc);
+  if (s == MCPET_OK) s = load_common(sc);
+  if (s != MCPET_OK) {
+    delete sc;
+    return s;
+  }
+  *out = sc;
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_scene_from_arrays(const mcpet_config* cfg, int nx, int ny, int nz, const float voxel_size_cm[3],
+                                     const int32_t* material, const float* density, const float* activity,
+                                     mcpet_scene** out) {
+  if (!out || !cfg) return set_error(MCPET_ERR_ARG, "null argument");
+  *out = nullptr;
+  mcpet_scene* sc = new (std::nothrow) mcpet_scene();
+  if (!sc) return set_error(MCPET_ERR_NOMEM, "out of host memory");
+  sc->cfg = *cfg;
+  if (sc->cfg.span <= 0) {
+    delete sc;
+    return set_error(MCPET_ERR_ARG, "SPAN must be positive");
+  }
+  derive_sinogram_sizes(&sc->cfg);
+  mcpet_status s = set_phantom_arrays(nx, ny, nz, voxel_size_cm, material, density, activity,
+                                      sc->cfg.density_factor, sc);
+  if (s == MCPET_OK) s = load_common(sc);
+  if (s != MCPET_OK) {
+    delete sc;
+    return s;
+  }
+  *out = sc;
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_scene_set_activity(mcpet_scene* sc, const float* activity) {
+  if (!sc || !activity) return set_error(MCPET_ERR_ARG, "null argument");
+  std::copy(activity, activity + sc->activity.size(), sc->activity.begin());
+  sc->dev.activity_dirty = true;
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_scene_get_config(const mcpet_scene* sc, mcpet_config* cfg) {
+  if (!sc || !cfg) return set_error(MCPET_ERR_ARG, "null argument");
+  *cfg = sc->cfg;
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_scene_get_info(const mcpet_scene* sc, mcpet_scene_info* info) {
+  if (!sc || !info) return set_error(MCPET_ERR_ARG, "null argument");
+  memset(info, 0, sizeof(*info));
+  info->nx = sc->nx;
+  info->ny = sc->ny;
+  info->nz = sc->nz;
+  for (int k = 0; k < 3; ++k) {
+    info->voxel_size[k] = sc->voxel_size[k];
+    info->bbox[k] = sc->bbox[k];
+  }
+  info->n_voxels = (long long)sc->mat0.size();
+  double tot = 0;
+  long long ne = 0;
+  for (float a : sc->activity)
+    if (a > 1.0e-7f) {
+      ne++;
+      tot += a;
+    }
+  info->n_emitting_voxels = ne;
+  info->total_activity_bq = tot;
+  info->n_energy = sc->n_e;
+  info->e0 = sc->e0;
+  info->inv_de = sc->ide;
+  int used = 0;
+  for (int m = 0; m < kMaxMaterials; ++m) {
+    if (sc->material_loaded[m]) used++;
+    info->density_max[m] = sc->density_max[m];
+    info->density_nominal[m] = sc->density_nominal[m];
+  }
+  info->n_materials_used = used;
+  info->n_palette = (int)sc->palette.size();
+  info->n_bins = sc->cfg.n_bins;
+  info->n_energy_spectrum = sc->cfg.n_energy_bins;
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_scene_export_tables(const mcpet_scene* sc, float* woodcock, float* mfp_a, float* mfp_b,
+                                       float* voxels, float* fco, float* uico, float* fj0, int32_t* noscco,
+                                       float* xco, float* pco, float* aco, float* bco, float* pmax, uint8_t* itlco,
+                                       uint8_t* ituco) {
+  if (!sc) return set_error(MCPET_ERR_ARG, "null scene");
+  if (woodcock) std::copy(sc->woodcock.begin(), sc->woodcock.end(), woodcock);
+  if (mfp_a) std::copy(sc->mfp_a.begin(), sc->mfp_a.end(), mfp_a);
+  if (mfp_b) std::copy(sc->mfp_b.begin(), sc->mfp_b.end(), mfp_b);
+  if (voxels)
+    for (size_t i = 0; i < sc->mat0.size(); ++i) {
+      voxels[3 * i + 0] = (float)(sc->mat0[i] + 1) + 0.0001f;
+      voxels[3 * i + 1] = sc->rho[i];
+      voxels[3 * i + 2] = sc->activity[i];
+    }
+  if (fco) memcpy(fco, sc->compton.fco, sizeof(sc->compton.fco));
+  if (uico) memcpy(uico, sc->compton.uico, sizeof(sc->compton.uico));
+  if (fj0) memcpy(fj0, sc->compton.fj0, sizeof(sc->compton.fj0));
+  if (noscco) memcpy(noscco, sc->compton.noscco, sizeof(sc->compton.noscco));
+  if (xco) std::copy(sc->xco.begin(), sc->xco.end(), xco);
+  if (pco) std::copy(sc->pco.begin(), sc->pco.end(), pco);
+  if (aco) std::copy(sc->aco.begin(), sc->aco.end(), aco);
+  if (bco) std::copy(sc->bco.begin(), sc->bco.end(), bco);
+  if (pmax) std::copy(sc->pmax.begin(), sc->pmax.end(), pmax);
+  if (itlco) std::copy(sc->itl.begin(), sc->itl.end(), itlco);
+  if (ituco) std::copy(sc->itu.begin(), sc->itu.end(), ituco);
+  return MCPET_OK;
+}
+
+void mcpet_scene_free(mcpet_scene* sc) { delete sc; }
+
+mcpet_status mcpet_scene_to_device(mcpet_scene* sc, int device) {
+  if (!sc) return set_error(MCPET_ERR_ARG, "null scene");
+  int dev = pick_device(device >= 0 ? device : sc->cfg.gpu_id);
+  if (dev < 0) return set_error(MCPET_ERR_CUDA, "no CUDA device available");
+  if (sc->dev.device >= 0 && sc->dev.device != dev)
+    return set_error(MCPET_ERR_ARG, "scene already bound to device %d", sc->dev.device);
+  CUDA_TRY(cudaSetDevice(dev));
+  sc->dev.device = dev;
+  int sms = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  sc->dev.sm_count = sms;
+  return upload_tables(sc);
+}
+
+mcpet_status mcpet_run_device(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out) {
+  if (!sc || !out) return set_error(MCPET_ERR_ARG, "null argument");
+  DeviceTallies O;
+  memset(&O, 0, sizeof(O));
+  O.trues = out->trues;
+  O.scatter = out->scatter;
+  O.image_trues = out->image_trues;
+  O.image_scatter = out->image_scatter;
+  O.spectrum = out->spectrum;
+  O.psf = (uint32_t*)out->psf;
+  O.psf_count = out->psf_count;
+  O.histories = out->total_histories;
+  O.counters = (unsigned long long*)out->counters;
+  cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
+  double ms = 0;
+  mcpet_status s = enqueue_run(sc, opts, O, st, out->transport_ms ? &ms : nullptr);
+  if (s == MCPET_OK && out->transport_ms) *out->transport_ms = ms;
+  return s;
+}
+
+mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out) {
+  if (!sc || !out) return set_error(MCPET_ERR_ARG, "null argument");
+  mcpet_status s = ensure_device(sc);
+  if (s != MCPET_OK) return s;
+  s = upload_tables(sc);
+  if (s != MCPET_OK) return s;
+  const bool want_psf = (sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 1) && out->psf;
+  s = ensure_run_buffers(sc, want_psf);
+  if (s != MCPET_OK) return s;
+  auto& d = sc->dev;
+  DeviceTallies O;
+  memset(&O, 0, sizeof(O));
+  O.trues = d.trues;
+  O.scatter = d.scatter;
+  O.image_trues = d.img_t;
+  O.image_scatter = d.img_s;
+  O.spectrum = d.spectrum;
+  O.psf = want_psf ? d.psf : nullptr;
+  O.histories = d.small + 2;
+  O.psf_count = (int*)(d.small + 3);
+  O.counters = (opts && opts->collect_counters) ? d.small + 4 : nullptr;
+  cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
+  double ms = 0;
+  s = enqueue_run(sc, opts, O, st, &ms);
+  if (s != MCPET_OK) return s;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
+  if (out->trues) CUDA_TRY(cudaMemcpyAsync(out->trues, d.trues, nb, cudaMemcpyDeviceToHost, st));
+  if (out->scatter) CUDA_TRY(cudaMemcpyAsync(out->scatter, d.scatter, nb, cudaMemcpyDeviceToHost, st));
+  if (out->image_trues) CUDA_TRY(cudaMemcpyAsync(out->image_trues, d.img_t, nv, cudaMemcpyDeviceToHost, st));
+  if (out->image_scatter) CUDA_TRY(cudaMemcpyAsync(out->image_scatter, d.img_s, nv, cudaMemcpyDeviceToHost, st));
+  if (out->spectrum)
+    CUDA_TRY(cudaMemcpyAsync(out->spectrum, d.spectrum, (size_t)sc->cfg.n_energy_bins * 4, cudaMemcpyDeviceToHost,
+                             st));
+  unsigned long long small[16];
+  CUDA_TRY(cudaMemcpyAsync(small, d.small, sizeof(small), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  int psf_count = (int)(small[3] & 0xffffffffull);
+  if (out->psf_count) *out->psf_count = psf_count;
+  if (out->total_histories) *out->total_histories = small[2];
+  if (want_psf) {
+    long long n = std::min<long long>(std::max(psf_count, 0), std::min<long long>(d.psf_cap, out->psf_capacity));
+    if (n > 0) CUDA_TRY(cudaMemcpy(out->psf, d.psf, (size_t)n * 44, cudaMemcpyDeviceToHost));
+  }
+  if (out->counters) {
+    memset(out->counters, 0, sizeof(mcpet_counters));
+    if (opts && opts->collect_counters) memcpy(out->counters, small + 4, 10 * 8);
+    out->counters->guard_trips = small[0];
+  }
+  if (out->transport_ms) *out->transport_ms = ms;
+  d.last_guard = small[0];
+  if (small[0] != 0)
+    return set_error(MCPET_ERR_DEVICE, "%llu device guard(s) fired (loop cap or out-of-range index)", small[0]);
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_last_run_guard(mcpet_scene* sc, unsigned long long* trips) {
+  if (!sc || !trips) return set_error(MCPET_ERR_ARG, "null argument");
+  if (sc->dev.device < 0 || !sc->dev.small) {
+    *trips = 0;
+    return MCPET_OK;
+  }
+  CUDA_TRY(cudaSetDevice(sc->dev.device));
+  CUDA_TRY(cudaMemcpy(trips, sc->dev.small, 8, cudaMemcpyDeviceToHost));
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_write_outputs(const mcpet_scene* sc, const mcpet_tallies* host, const char* out_dir,
+                                 int background_mode, double elapsed_s) {
+  if (!sc || !host) return set_error(MCPET_ERR_ARG, "null argument");
+  return write_outputs(sc, host, out_dir, background_mode, elapsed_s);
+}
+
+}  // extern "C"
+
+/* ------------------------------------------------------------- probes */
+
+namespace {
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t n, const void* src = nullptr) {
+    cudaError_t e = cudaMalloc((void**)&p, sizeof(T) * (n ? n : 1));
+    if (e != cudaSuccess) return e;
+    if (src) return cudaMemcpy(p, src, sizeof(T) * n, cudaMemcpyHostToDevice);
+    return cudaMemset(p, 0, sizeof(T) * (n ? n : 1));
+  }
+};
+mcpet_status probe_device() {
+  int d = pick_device(-1);
+  if (d < 0) return set_error(MCPET_ERR_CUDA, "no CUDA device available");
+  CUDA_TRY(cudaSetDevice(d));
+  return MCPET_OK;
+}
+}  // namespace
+
+extern "C" {
+
+mcpet_status mcpet_probe_rng(int n, int seed_input, const int64_t* stream_ids, int ndraw, int32_t* seeds_out,
+                             float* draws, double* ddraws) {
+  if (n <= 0 || !stream_ids || !seeds_out || ndraw < 0 || (ndraw > 0 && (!draws || !ddraws)))
+    return set_error(MCPET_ERR_ARG, "invalid probe arguments");
+  if (seed_input <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive");
+  mcpet_status s = probe_device();
+  if (s != MCPET_OK) return s;
+  TransportParams P;
+  memset(&P, 0, sizeof(P));
+  jump_tables(P.jump1, P.jump2);
+  P.seed = seed_input;
+  DBuf<int64_t> ids;
+  DBuf<int2> sd;
+  DBuf<float> f;
+  DBuf<double> dd;
+  CUDA_TRY(ids.alloc(n, stream_ids));
+  CUDA_TRY(sd.alloc(n));
+  CUDA_TRY(f.alloc((size_t)n * ndraw));
+  CUDA_TRY(dd.alloc((size_t)n * ndraw));
+  CUDA_TRY(launch_probe_rng(P, n, ids.p, ndraw, sd.p, f.p, dd.p, nullptr));
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(seeds_out, sd.p, sizeof(int2) * n, cudaMemcpyDeviceToHost));
+  if (ndraw > 0) {
+    CUDA_TRY(cudaMemcpy(draws, f.p, sizeof(float) * n * ndraw, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(ddraws, dd.p, sizeof(double) * n * ndraw, cudaMemcpyDeviceToHost));
+  }
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_probe_detector(const mcpet_scene* sc, int n, const float* e2, const float* e1, const float* pos2,
+                                  const float* pos1, const float* dir2, const float* dir1, const int8_t* st2,
+                                  const int8_t* st1, const int32_t* seeds, int32_t* out) {
+  if (!sc || n <= 0 || !e2 || !e1 || !pos2 || !pos1 || !dir2 || !dir1 || !st2 || !st1 || !seeds || !out)
+    return set_error(MCPET_ERR_ARG, "invalid probe arguments");
+  mcpet_status s = probe_device();
+  if (s != MCPET_OK) return s;
+  TransportParams P;
+  fill_params(sc, P);
+  DBuf<float> de2, de1;
+  DBuf<float3> dp2, dp1, dd2, dd1;
+  DBuf<int8_t> ds2, ds1;
+  DBuf<int2> dsd;
+  DBuf<int> dout;
+  CUDA_TRY(de2.alloc(n, e2));
+  CUDA_TRY(de1.alloc(n, e1));
+  CUDA_TRY(dp2.alloc(n, pos2));
+  CUDA_TRY(dp1.alloc(n, pos1));
+  CUDA_TRY(dd2.alloc(n, dir2));
+  CUDA_TRY(dd1.alloc(n, dir1));
+  CUDA_TRY(ds2.alloc(n, st2));
+  CUDA_TRY(ds1.alloc(n, st1));
+  CUDA_TRY(dsd.alloc(n, seeds));
+  CUDA_TRY(dout.alloc((size_t)6 * n));
+  CUDA_TRY(launch_probe_detector(P, n, de2.p, de1.p, dp2.p, dp1.p, dd2.p, dd1.p, ds2.p, ds1.p, dsd.p, dout.p,
+                                 nullptr));
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(out, dout.p, sizeof(int) * 6 * n, cudaMemcpyDeviceToHost));
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_probe_compton(const mcpet_scene* sc, int n, const float* energy_in, const int32_t* mat,
+                                 const int32_t* seeds_in, float* energy_out, double* costh_out, int32_t* seeds_out) {
+  if (!sc || n <= 0 || !energy_in || !mat || !seeds_in || !energy_out || !costh_out || !seeds_out)
+    return set_error(MCPET_ERR_ARG, "invalid probe arguments");
+  for (int i = 0; i < n; ++i)
+    if (mat[i] < 0 || mat[i] >= kMaxMaterials || !sc->material_loaded[mat[i]])
+      return set_error(MCPET_ERR_ARG, "material %d not loaded", mat[i]);
+  mcpet_status s = probe_device();
+  if (s != MCPET_OK) return s;
+  DBuf<ComptonTable> tab;
+  DBuf<float> de;
+  DBuf<int> dm;
+  DBuf<int2> dsd;
+  DBuf<double> dc;
+  CUDA_TRY(tab.alloc(1, &sc->compton));
+  CUDA_TRY(de.alloc(n, energy_in));
+  CUDA_TRY(dm.alloc(n, mat));
+  CUDA_TRY(dsd.alloc(n, seeds_in));
+  CUDA_TRY(dc.alloc(n));
+  CUDA_TRY(launch_probe_compton(tab.p, n, de.p, dm.p, dsd.p, dc.p, nullptr));
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(energy_out, de.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(costh_out, dc.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(seeds_out, dsd.p, sizeof(int2) * n, cudaMemcpyDeviceToHost));
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_probe_rayleigh(const mcpet_scene* sc, int n, const float* energy_in, const int32_t* mat,
+                                  const float* pmax, const int32_t* seeds_in, double* costh_out, int32_t* seeds_out) {
+  if (!sc || n <= 0 || !energy_in || !mat || !pmax || !seeds_in || !costh_out || !seeds_out)
+    return set_error(MCPET_ERR_ARG, "invalid probe arguments");
+  for (int i = 0; i < n; ++i)
+    if (mat[i] < 0 || mat[i] >= kMaxMaterials || !sc->material_loaded[mat[i]])
+      return set_error(MCPET_ERR_ARG, "material %d not loaded", mat[i]);
+  mcpet_status s = probe_device();
+  if (s != MCPET_OK) return s;
+  const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
+  std::vector<float> ray(4 * nr);
+  std::copy(sc->xco.begin(), sc->xco.end(), ray.begin());
+  std::copy(sc->pco.begin(), sc->pco.end(), ray.begin() + nr);
+  std::copy(sc->aco.begin(), sc->aco.end(), ray.begin() + 2 * nr);
+  std::copy(sc->bco.begin(), sc->bco.end(), ray.begin() + 3 * nr);
+  std::vector<uint8_t> r8(2 * nr);
+  std::copy(sc->itl.begin(), sc->itl.end(), r8.begin());
+  std::copy(sc->itu.begin(), sc->itu.end(), r8.begin() + nr);
+  DBuf<float> dray, de, dp;
+  DBuf<uint8_t> dr8;
+  DBuf<int> dm;
+  DBuf<int2> dsd;
+  DBuf<double> dc;
+  CUDA_TRY(dray.alloc(4 * nr, ray.data()));
+  CUDA_TRY(dr8.alloc(2 * nr, r8.data()));
+  CUDA_TRY(de.alloc(n, energy_in));
+  CUDA_TRY(dm.alloc(n, mat));
+  CUDA_TRY(dp.alloc(n, pmax));
+  CUDA_TRY(dsd.alloc(n, seeds_in));
+  CUDA_TRY(dc.alloc(n));
+  RayleighRows R{dray.p, dray.p + nr, dray.p + 2 * nr, dray.p + 3 * nr, dr8.p, dr8.p + nr};
+  CUDA_TRY(launch_probe_rayleigh(R, n, de.p, dm.p, dp.p, dsd.p, dc.p, nullptr));
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(costh_out, dc.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(seeds_out, dsd.p, sizeof(int2) * n, cudaMemcpyDeviceToHost));
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_probe_source(int nx, int ny, int nz, const float inv_voxel_size[3], int background_mode,
+                                const int32_t* seeds_in, float* out, int32_t* seeds_out) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || !inv_voxel_size || !seeds_in || !out || !seeds_out)
+    return set_error(MCPET_ERR_ARG, "invalid probe arguments");
+  mcpet_status s = probe_device();
+  if (s != MCPET_OK) return s;
+  TransportParams P;
+  memset(&P, 0, sizeof(P));
+  P.nx = nx;
+  P.ny = ny;
+  P.nz = nz;
+  P.inv_vx = inv_voxel_size[0];
+  P.inv_vy = inv_voxel_size[1];
+  P.inv_vz = inv_voxel_size[2];
+  P.n_voxels = (long long)nx * ny * nz;
+  DBuf<int2> dsd;
+  DBuf<float3> dout;
+  CUDA_TRY(dsd.alloc(P.n_voxels, seeds_in));
+  CUDA_TRY(dout.alloc(4 * P.n_voxels));
+  CUDA_TRY(launch_probe_source(P, background_mode, dsd.p, dout.p, nullptr));
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpy(out, dout.p, sizeof(float3) * 4 * P.n_voxels, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(seeds_out, dsd.p, sizeof(int2) * P.n_voxels, cudaMemcpyDeviceToHost));
+  return MCPET_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,29 @@
+/* Launch wrappers of the transport and probe kernels (host side). */
+#pragma once
+#include <cuda_runtime_api.h>
+#include <vector_types.h>
+#include <stddef.h>
+#include <stdint.h>
+#include "mcpet_params.h"
+
+namespace mcpet {
+
+size_t transport_dynamic_smem(const TransportParams& P, int block);
+int transport_block_threads();
+cudaError_t transport_occupancy(bool counters, int block, size_t smem, int* blocks_per_sm);
+cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
+                             bool counters, int grid, int block, size_t smem, cudaStream_t stream);
+
+cudaError_t launch_probe_rng(const TransportParams& P, int n, const int64_t* ids, int ndraw, int2* seeds,
+                             float* draws, double* ddraws, cudaStream_t s);
+cudaError_t launch_probe_detector(const TransportParams& P, int n, const float* e2, const float* e1,
+                                  const float3* p2, const float3* p1, const float3* d2, const float3* d1,
+                                  const int8_t* s2, const int8_t* s1, int2* seeds, int* out, cudaStream_t s);
+cudaError_t launch_probe_compton(const ComptonTable* tab, int n, float* energy, const int* mat, int2* seeds,
+                                 double* costh, cudaStream_t s);
+cudaError_t launch_probe_rayleigh(const RayleighRows& R, int n, const float* energy, const int* mat,
+                                  const float* pmax, int2* seeds, double* costh, cudaStream_t s);
+cudaError_t launch_probe_source(const TransportParams& P, int background, int2* seeds, float3* out,
+                                cudaStream_t s);
+
+}  // namespace mcpet

@@ -1,0 +1,123 @@
+/* Plain-old-data structures shared by the host library (C++) and the CUDA
+ * kernels.  Compiled by both g++ and nvcc. */
+#pragma once
+#include <stdint.h>
+
+namespace mcpet {
+
+constexpr int kMaxMaterials = 15;     /* MCGPU-PET.h:96 */
+constexpr int kMaxShells = 30;        /* MCGPU-PET.h:97 */
+constexpr int kNpRayleigh = 128;      /* MCGPU-PET.h:98 */
+constexpr int kMaxEnergyBins = 25005; /* MCGPU-PET.h:99 */
+constexpr int kLeapHistories = 555555;  /* histories_per_thread of the jump, MCGPU-PET_kernel.cu:252 */
+constexpr int kLeapDistance = 256;      /* LEAP_DISTANCE, MCGPU-PET_kernel.cu:898 */
+constexpr int kSpectrumSharedMax = 4096; /* spectrum bins privatised in shared memory */
+
+/* Interaction record for one (energy bin, material): the interpolation
+ * coefficients of the three inverse mean free paths (total, Compton,
+ * Rayleigh; reference mfp_table_a/b, MCGPU-PET.cu:1688-1746) interleaved with
+ * the Rayleigh form-factor maximum of the NEXT energy bin (the value GRAa is
+ * called with, MCGPU-PET_kernel.cu:379).  32 bytes = one sector, fetched with
+ * two 16-byte loads. */
+struct alignas(16) MfpRecord {
+  float ax, bx, ay, by;
+  float az, bz, pmax_next, pad;
+};
+
+/* Distinct (material, density) pair of the phantom; voxels store an index. */
+struct PaletteEntry {
+  int32_t mat0;     /* 0-based material */
+  float rho;        /* density g/cm^3 (already scaled by the density factor) */
+};
+
+/* Compton shell data (PENELOPE /CGCO/, reference compton_struct). */
+struct ComptonTable {
+  float fco[kMaxShells * kMaxMaterials];
+  float uico[kMaxShells * kMaxMaterials];
+  float fj0[kMaxShells * kMaxMaterials];
+  int32_t noscco[kMaxMaterials];
+};
+
+/* Rayleigh RITA sampling rows (PENELOPE /CGRA/), indexed [mat*128 + i]. */
+struct RayleighRows {
+  const float* xco;
+  const float* pco;
+  const float* aco;
+  const float* bco;
+  const uint8_t* itl;
+  const uint8_t* itu;
+};
+
+/* One emitting voxel of the lane plan.  Lanes [first_lane, first_lane+n)
+ * belong to it; lane k of it uses RANECU stream stream_base + k. */
+struct Emitter {
+  double inv_rate;        /* lanes/activity  (reference: blockDim.x/activity, MCGPU-PET_kernel.cu:233) */
+  uint32_t voxel;         /* linear voxel index (x fastest) */
+  uint32_t n_lanes;
+  uint64_t first_lane;
+  uint64_t stream_base;
+};
+
+/* Everything a transport launch needs by value (kernel parameter space). */
+struct TransportParams {
+  /* voxel grid (voxel_struct, MCGPU-PET.h:262-271) */
+  int nx, ny, nz;
+  float inv_vx, inv_vy, inv_vz;
+  float bbx, bby, bbz;
+  long long n_voxels;
+  /* energy grid (linear_interp) */
+  int n_e;
+  float e0, ide;
+  /* detector (detector_struct) */
+  float cx, cy, cz, radius, height;
+  int psf_capacity;
+  int tally_psf_sinogram, tally_type;
+  /* source */
+  unsigned long long acq_ps;
+  double inv_mean_life;
+  int background_mode;
+  /* sinogram and energy window */
+  float e_resol, e_low, e_high, fovz;
+  int nrows, ncrystals, nangles, nrad, nzs, ne, mrd, span, nsinos;
+  long long nbins;
+  /* RANECU jump tables: (a^(555555*256))^(2^k) mod m, k = 0..31 */
+  int32_t jump1[32];
+  int32_t jump2[32];
+  int seed;
+  /* lane plan */
+  uint64_t n_lanes;
+  int n_emitters;
+  int palette_in_shared;  /* palette size if staged in shared memory, else 0 */
+  int spectrum_in_shared; /* 1 when ne <= kSpectrumSharedMax */
+  int max_shells;         /* largest noscco over used materials */
+};
+
+/* Device pointers of one scene (all read-only during transport). */
+struct DeviceTables {
+  const uint16_t* vox16;          /* palette index per voxel when n_palette <= 65536 */
+  const uint32_t* vox32;          /* palette index per voxel otherwise */
+  const PaletteEntry* palette;
+  int n_palette;
+  const float* woodcock;          /* float2[n_e]: majorant mfp = x + E*y */
+  const MfpRecord* mfp;           /* [n_e * 15] */
+  const ComptonTable* compton;
+  RayleighRows rayleigh;
+  const Emitter* emitters;        /* [n_emitters], ordered by decreasing lane work */
+};
+
+/* Device pointers of the outputs of one run. */
+struct DeviceTallies {
+  int* trues;
+  int* scatter;
+  int* image_trues;
+  int* image_scatter;
+  int* spectrum;
+  uint32_t* psf;                  /* 11 words per packed 44-byte record */
+  int* psf_count;
+  unsigned long long* histories;
+  unsigned long long* counters;   /* 10 counters (mcpet_counters order) or NULL */
+  unsigned long long* guard;      /* guard trips */
+  unsigned long long* lane_cursor;/* lane work queue head */
+};
+
+}  // namespace mcpet

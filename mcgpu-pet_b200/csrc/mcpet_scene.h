@@ -1,0 +1,95 @@
+/* Host-side scene of the transport path: parsed configuration, phantom,
+ * interpolation tables in the reference layout, and the device copy. */
+#pragma once
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "mcpet.h"
+#include "mcpet_params.h"
+
+struct mcpet_scene {
+  mcpet_config cfg;
+
+  /* phantom (load_voxels, MCGPU-PET.cu:1381-1533) */
+  int nx = 0, ny = 0, nz = 0;
+  float voxel_size[3] = {0, 0, 0};
+  float inv_voxel_size[3] = {0, 0, 0};
+  float bbox[3] = {0, 0, 0};
+  std::vector<int32_t> mat0;      /* 0-based material per voxel */
+  std::vector<float> rho;         /* density per voxel, scaled by the density factor */
+  std::vector<float> activity;    /* Bq per voxel */
+  float density_max[mcpet::kMaxMaterials];
+  float density_nominal[mcpet::kMaxMaterials];
+
+  /* tables (load_material, MCGPU-PET.cu:1565-1831) in the reference layout */
+  int n_e = 0;
+  float e0 = 0.f, ide = 0.f;
+  double delta_e = 0.0;
+  std::vector<float> woodcock;    /* float2[n_e] */
+  std::vector<float> mfp_a, mfp_b;/* float3[n_e*15] */
+  std::vector<float> pmax;        /* [n_e*15] */
+  mcpet::ComptonTable compton;
+  std::vector<float> xco, pco, aco, bco;   /* [15*128] */
+  std::vector<uint8_t> itl, itu;
+  bool material_loaded[mcpet::kMaxMaterials];
+
+  /* palette compression of (material, density) */
+  std::vector<mcpet::PaletteEntry> palette;
+  std::vector<uint32_t> voxel_key;
+
+  /* device copy */
+  struct Device {
+    int device = -1;
+    bool tables_ready = false;
+    bool activity_dirty = true;
+    int sm_count = 0;
+    void* vox = nullptr;          /* uint16 or uint32 keys */
+    bool vox16 = true;
+    mcpet::PaletteEntry* palette = nullptr;
+    float* woodcock = nullptr;
+    mcpet::MfpRecord* mfp = nullptr;
+    mcpet::ComptonTable* compton = nullptr;
+    float* ray = nullptr;         /* xco|pco|aco|bco contiguous */
+    uint8_t* ray8 = nullptr;      /* itl|itu contiguous */
+    mcpet::Emitter* emitters = nullptr;
+    size_t emitters_cap = 0;
+    int n_emitters = 0;
+    uint64_t n_lanes = 0;
+    std::string plan_key;
+    /* run scratch owned by the scene (host-buffer runs) */
+    int* trues = nullptr;
+    int* scatter = nullptr;
+    int* img_t = nullptr;
+    int* img_s = nullptr;
+    int* spectrum = nullptr;
+    uint32_t* psf = nullptr;
+    long long psf_cap = 0;
+    unsigned long long* small = nullptr;  /* histories, guard, cursor, psf_count, 10 counters */
+    long long nbins_alloc = -1, nvox_alloc = -1;
+    int ne_alloc = -1;
+    void* ev0 = nullptr;
+    void* ev1 = nullptr;
+    unsigned long long last_guard = 0;
+  } dev;
+
+  ~mcpet_scene();
+};
+
+namespace mcpet {
+
+/* thread-local error text */
+mcpet_status set_error(mcpet_status s, const char* fmt, ...);
+
+/* mcpet_io.cpp */
+mcpet_status parse_input(const char* in_path, mcpet_config* cfg);
+mcpet_status load_phantom_file(const char* path, float density_factor, mcpet_scene* sc);
+mcpet_status set_phantom_arrays(int nx, int ny, int nz, const float vs[3], const int32_t* material,
+                                const float* density, const float* activity, float density_factor,
+                                mcpet_scene* sc);
+mcpet_status load_materials(mcpet_scene* sc);
+mcpet_status finalize_scene(mcpet_scene* sc);
+mcpet_status write_outputs(const mcpet_scene* sc, const mcpet_tallies* t, const char* out_dir, int bg,
+                           double elapsed_s);
+void derive_sinogram_sizes(mcpet_config* cfg);
+
+}  // namespace mcpet

@@ -1,0 +1,335 @@
+"""Python view of the C ABI: scenes, runs, outputs and verification probes.
+
+This is the thin test/benchmark binding over ``libmcpet.so``; every call goes
+through the C ABI of include/mcpet.h.  Host results come back as numpy
+arrays; device runs take torch CUDA tensors (used for device-resident timing).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, lib
+
+
+def _ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays passed to the C ABI must be contiguous"
+    return a.ctypes.data
+
+
+@dataclass
+class RunOptions:
+    """Options of one transport run (mcpet_run_opts)."""
+
+    lane_mode: int = _abi.LANES_REFERENCE
+    background_mode: bool = False
+    histories_per_lane: int = 0
+    block_threads: int = 0
+    blocks_per_sm: int = 0
+    collect_counters: bool = False
+    seed_override: int = 0
+    stream: int = 0
+
+    def to_c(self) -> _abi.RunOpts:
+        o = _abi.RunOpts()
+        o.lane_mode = int(self.lane_mode)
+        o.background_mode = int(bool(self.background_mode))
+        o.histories_per_lane = int(self.histories_per_lane)
+        o.block_threads = int(self.block_threads)
+        o.blocks_per_sm = int(self.blocks_per_sm)
+        o.collect_counters = int(bool(self.collect_counters))
+        o.seed_override = int(self.seed_override)
+        o.stream = self.stream or None
+        return o
+
+
+@dataclass
+class RunResult:
+    trues: Optional[np.ndarray]
+    scatter: Optional[np.ndarray]
+    image_trues: Optional[np.ndarray]
+    image_scatter: Optional[np.ndarray]
+    spectrum: np.ndarray
+    psf: Optional[np.ndarray]          # structured array of PSF records
+    psf_count: int
+    total_histories: int
+    transport_ms: float
+    counters: dict = field(default_factory=dict)
+
+    @property
+    def coincidences(self) -> int:
+        t = 0 if self.trues is None else int(self.trues.sum(dtype=np.int64))
+        s = 0 if self.scatter is None else int(self.scatter.sum(dtype=np.int64))
+        return t + s
+
+
+PSF_DTYPE = np.dtype(
+    [
+        ("emission_time_ps", "<u8"),
+        ("travel_time_ps", "<f4"),
+        ("emission_absvox", "<i4"),
+        ("energy", "<f4"),
+        ("z", "<f4"),
+        ("phi", "<f4"),
+        ("vx", "<f4"),
+        ("vy", "<f4"),
+        ("vz", "<f4"),
+        ("index1", "<i2"),
+        ("index2", "<i2"),
+    ]
+)
+assert PSF_DTYPE.itemsize == _abi.PSF_RECORD_BYTES
+
+
+def read_config(in_path: str) -> _abi.Config:
+    cfg = _abi.Config()
+    check(lib().mcpet_config_read(os.fsencode(in_path), C.byref(cfg)))
+    return cfg
+
+
+class Scene:
+    """A loaded phantom + material tables (+ its device copy)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    # -- construction ------------------------------------------------------
+    @classmethod
+    def load(cls, in_path: str) -> "Scene":
+        h = C.c_void_p()
+        check(lib().mcpet_scene_load(os.fsencode(in_path), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, cfg: _abi.Config, material: np.ndarray, density: np.ndarray, activity: np.ndarray,
+                    voxel_size_cm) -> "Scene":
+        """Arrays shaped (nz, ny, nx) (x fastest in memory), material 1-based."""
+        material = np.ascontiguousarray(material, dtype=np.int32)
+        density = np.ascontiguousarray(density, dtype=np.float32)
+        activity = np.ascontiguousarray(activity, dtype=np.float32)
+        nz, ny, nx = material.shape
+        vs = np.ascontiguousarray(voxel_size_cm, dtype=np.float32)
+        h = C.c_void_p()
+        check(lib().mcpet_scene_from_arrays(C.byref(cfg), nx, ny, nz, _ptr(vs), _ptr(material), _ptr(density),
+                                            _ptr(activity), C.byref(h)))
+        return cls(h.value)
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().mcpet_scene_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- queries -----------------------------------------------------------
+    @property
+    def config(self) -> _abi.Config:
+        cfg = _abi.Config()
+        check(lib().mcpet_scene_get_config(self._h, C.byref(cfg)))
+        return cfg
+
+    @property
+    def info(self) -> _abi.SceneInfo:
+        info = _abi.SceneInfo()
+        check(lib().mcpet_scene_get_info(self._h, C.byref(info)))
+        return info
+
+    def set_activity(self, activity: np.ndarray) -> None:
+        a = np.ascontiguousarray(activity, dtype=np.float32).ravel()
+        assert a.size == self.info.n_voxels
+        check(lib().mcpet_scene_set_activity(self._h, _ptr(a)))
+
+    def export_tables(self) -> dict:
+        """Host tables in the reference layout (for parity checks)."""
+        info = self.info
+        ne, nv = info.n_energy, info.n_voxels
+        M, S, R = _abi.MAX_MATERIALS, _abi.MAX_SHELLS, _abi.NP_RAYLEIGH
+        t = {
+            "woodcock": np.zeros((ne, 2), np.float32),
+            "mfp_a": np.zeros((ne, M, 3), np.float32),
+            "mfp_b": np.zeros((ne, M, 3), np.float32),
+            "voxels": np.zeros((nv, 3), np.float32),
+            "fco": np.zeros(S * M, np.float32),
+            "uico": np.zeros(S * M, np.float32),
+            "fj0": np.zeros(S * M, np.float32),
+            "noscco": np.zeros(M, np.int32),
+            "xco": np.zeros(M * R, np.float32),
+            "pco": np.zeros(M * R, np.float32),
+            "aco": np.zeros(M * R, np.float32),
+            "bco": np.zeros(M * R, np.float32),
+            "pmax": np.zeros((ne, M), np.float32),
+            "itlco": np.zeros(M * R, np.uint8),
+            "ituco": np.zeros(M * R, np.uint8),
+        }
+        order = ["woodcock", "mfp_a", "mfp_b", "voxels", "fco", "uico", "fj0", "noscco", "xco", "pco", "aco", "bco",
+                 "pmax", "itlco", "ituco"]
+        check(lib().mcpet_scene_export_tables(self._h, *[_ptr(t[k]) for k in order]))
+        return t
+
+    # -- runs ----------------------------------------------------------------
+    def to_device(self, device: int = -1) -> None:
+        check(lib().mcpet_scene_to_device(self._h, device))
+
+    def run(self, opts: Optional[RunOptions] = None, psf_capacity: Optional[int] = None) -> RunResult:
+        """End-to-end run into host (numpy) buffers (mcpet_run)."""
+        opts = opts or RunOptions()
+        cfg, info = self.config, self.info
+        sino = cfg.tally_psf_sinogram in (0, 2)
+        want_psf = cfg.tally_psf_sinogram in (0, 1)
+        nb, nv = int(cfg.n_bins), int(info.n_voxels)
+        trues = np.zeros(nb, np.int32) if sino else None
+        scatter = np.zeros(nb, np.int32) if sino else None
+        img_t = np.zeros(nv, np.int32) if sino else None
+        img_s = np.zeros(nv, np.int32) if sino else None
+        spec = np.zeros(max(cfg.n_energy_bins, 1), np.int32)
+        cap = int(cfg.psf_size if psf_capacity is None else psf_capacity) if want_psf else 0
+        psf = np.zeros(cap, PSF_DTYPE) if cap > 0 else None
+        psf_count = C.c_int32(0)
+        hist = C.c_ulonglong(0)
+        ms = C.c_double(0)
+        cnt = _abi.Counters()
+        t = _abi.Tallies()
+        t.trues, t.scatter, t.image_trues, t.image_scatter = _ptr(trues), _ptr(scatter), _ptr(img_t), _ptr(img_s)
+        t.spectrum = _ptr(spec)
+        t.psf = _ptr(psf) if psf is not None else None
+        t.psf_capacity = cap
+        t.psf_count = C.addressof(psf_count)
+        t.total_histories = C.addressof(hist)
+        t.counters = C.addressof(cnt)
+        t.transport_ms = C.addressof(ms)
+        co = opts.to_c()
+        check(lib().mcpet_run(self._h, C.byref(co), C.byref(t)))
+        n = psf_count.value
+        counters = {name: int(getattr(cnt, name)) for name, _ in _abi.Counters._fields_}
+        return RunResult(trues, scatter, img_t, img_s, spec,
+                         psf[: max(0, min(n, cap))] if psf is not None else None, n, int(hist.value),
+                         float(ms.value), counters)
+
+    def run_device(self, tallies: dict, opts: Optional[RunOptions] = None, time_it: bool = False) -> float:
+        """Run into caller-owned torch CUDA tensors (mcpet_run_device).
+
+        ``tallies`` holds int32 tensors trues/scatter/image_trues/image_scatter/
+        spectrum, an int32 psf_count[1] and an int64 histories[1] (optionally
+        a uint8 psf[capacity*44] and int64 counters[10]).  Returns the
+        transport time in ms when ``time_it`` (this synchronises)."""
+        opts = opts or RunOptions()
+
+        def p(name):
+            x = tallies.get(name)
+            return None if x is None else x.data_ptr()
+
+        ms = C.c_double(0)
+        t = _abi.Tallies()
+        t.trues, t.scatter = p("trues"), p("scatter")
+        t.image_trues, t.image_scatter = p("image_trues"), p("image_scatter")
+        t.spectrum = p("spectrum")
+        t.psf = p("psf")
+        t.psf_capacity = 0 if tallies.get("psf") is None else tallies["psf"].numel() // _abi.PSF_RECORD_BYTES
+        t.psf_count = p("psf_count")
+        t.total_histories = p("histories")
+        t.counters = p("counters")
+        t.transport_ms = C.addressof(ms) if time_it else None
+        co = opts.to_c()
+        check(lib().mcpet_run_device(self._h, C.byref(co), C.byref(t)))
+        return float(ms.value)
+
+    def guard_trips(self) -> int:
+        v = C.c_ulonglong(0)
+        check(lib().mcpet_last_run_guard(self._h, C.byref(v)))
+        return int(v.value)
+
+    def write_outputs(self, result: RunResult, out_dir: Optional[str] = None, background_mode: bool = False) -> None:
+        t = _abi.Tallies()
+        t.trues, t.scatter = _ptr(result.trues), _ptr(result.scatter)
+        t.image_trues, t.image_scatter = _ptr(result.image_trues), _ptr(result.image_scatter)
+        t.spectrum = _ptr(result.spectrum)
+        psf_count = C.c_int32(result.psf_count)
+        hist = C.c_ulonglong(result.total_histories)
+        if result.psf is not None:
+            t.psf = _ptr(result.psf)
+            t.psf_capacity = len(result.psf)
+        t.psf_count = C.addressof(psf_count)
+        t.total_histories = C.addressof(hist)
+        check(lib().mcpet_write_outputs(self._h, C.byref(t), os.fsencode(out_dir) if out_dir else None,
+                                        int(bool(background_mode)), result.transport_ms * 1e-3))
+
+
+# -- verification probes (GPU) -----------------------------------------------
+
+def probe_rng(seed: int, stream_ids, ndraw: int = 8):
+    ids = np.ascontiguousarray(stream_ids, dtype=np.int64)
+    n = len(ids)
+    seeds = np.zeros((n, 2), np.int32)
+    f = np.zeros((n, ndraw), np.float32)
+    d = np.zeros((n, ndraw), np.float64)
+    check(lib().mcpet_probe_rng(n, int(seed), _ptr(ids), ndraw, _ptr(seeds), _ptr(f), _ptr(d)))
+    return seeds, f, d
+
+
+def probe_detector(scene: Scene, ev: dict) -> np.ndarray:
+    n = len(ev["e2"])
+    a = {k: np.ascontiguousarray(ev[k], dtype=(np.int8 if k.startswith("st") else
+                                               np.int32 if k == "seeds" else np.float32)) for k in
+         ["e2", "e1", "pos2", "pos1", "dir2", "dir1", "st2", "st1", "seeds"]}
+    out = np.zeros((n, 6), np.int32)
+    check(lib().mcpet_probe_detector(scene.handle, n, _ptr(a["e2"]), _ptr(a["e1"]), _ptr(a["pos2"]),
+                                     _ptr(a["pos1"]), _ptr(a["dir2"]), _ptr(a["dir1"]), _ptr(a["st2"]),
+                                     _ptr(a["st1"]), _ptr(a["seeds"]), _ptr(out)))
+    return out
+
+
+def probe_compton(scene: Scene, energy, mat, seeds):
+    e = np.ascontiguousarray(energy, np.float32)
+    m = np.ascontiguousarray(mat, np.int32)
+    s = np.ascontiguousarray(seeds, np.int32).reshape(-1, 2)
+    n = len(e)
+    e_out = np.zeros(n, np.float32)
+    c_out = np.zeros(n, np.float64)
+    s_out = np.zeros((n, 2), np.int32)
+    check(lib().mcpet_probe_compton(scene.handle, n, _ptr(e), _ptr(m), _ptr(s), _ptr(e_out), _ptr(c_out),
+                                    _ptr(s_out)))
+    return e_out, c_out, s_out
+
+
+def probe_rayleigh(scene: Scene, energy, mat, pmax, seeds):
+    e = np.ascontiguousarray(energy, np.float32)
+    m = np.ascontiguousarray(mat, np.int32)
+    p = np.ascontiguousarray(pmax, np.float32)
+    s = np.ascontiguousarray(seeds, np.int32).reshape(-1, 2)
+    n = len(e)
+    c_out = np.zeros(n, np.float64)
+    s_out = np.zeros((n, 2), np.int32)
+    check(lib().mcpet_probe_rayleigh(scene.handle, n, _ptr(e), _ptr(m), _ptr(p), _ptr(s), _ptr(c_out),
+                                     _ptr(s_out)))
+    return c_out, s_out
+
+
+def probe_source(shape, inv_voxel_size, seeds, background: bool = False):
+    nz, ny, nx = shape
+    inv = np.ascontiguousarray(inv_voxel_size, np.float32)
+    s = np.ascontiguousarray(seeds, np.int32).reshape(-1, 2)
+    out = np.zeros((nx * ny * nz, 4, 3), np.float32)
+    s_out = np.zeros_like(s)
+    check(lib().mcpet_probe_source(nx, ny, nz, _ptr(inv), int(bool(background)), _ptr(s), _ptr(out), _ptr(s_out)))
+    return out, s_out
