@@ -112,6 +112,9 @@ typedef struct {
   float density_nominal[MCPET_MAX_MATERIALS];
   long long n_bins;
   int n_energy_spectrum;
+  int n_emitters;                 /* lane plan of the last run */
+  long long n_lanes;
+  long long last_h2d_bytes;       /* bytes copied host->device by the last run */
 } mcpet_scene_info;
 
 typedef struct {
@@ -149,6 +152,7 @@ typedef struct {
   long long psf_capacity;         /* elements; the reference's PSF_size */
   int32_t* psf_count;             /* the reference's index_PSF after the run */
   unsigned long long* total_histories;  /* photons (2 per decay), MCGPU-PET_kernel.cu:282 */
+  unsigned long long* coincidences;     /* detected pairs = sum(trues) + sum(scatter) */
   mcpet_counters* counters;
   double* transport_ms;           /* device time of the transport kernel(s) */
 } mcpet_tallies;

@@ -173,6 +173,9 @@ mcpet_status upload_tables(mcpet_scene* sc) {
   CUDA_TRY(dmalloc(&d.ray8, 2 * nr));
   CUDA_TRY(cudaMemcpy(d.ray8, r8.data(), 2 * nr, cudaMemcpyHostToDevice));
   CUDA_TRY(dmalloc(&d.small, 16 * sizeof(unsigned long long)));
+  d.run_h2d += (long long)(nv * (d.vox16 ? 2 : 4) + sc->palette.size() * sizeof(PaletteEntry) +
+                           sc->woodcock.size() * 4 + nrec * sizeof(MfpRecord) + sizeof(ComptonTable) + 4 * nr * 4 +
+                           2 * nr);
   cudaEvent_t e0, e1;
   CUDA_TRY(cudaEventCreate(&e0));
   CUDA_TRY(cudaEventCreate(&e1));
@@ -212,6 +215,7 @@ mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
   char key[128];
   snprintf(key, sizeof(key), "%d/%d/%d", mode, tpb, hpl);
   if (!d.activity_dirty && d.plan_key == key && d.emitters) return MCPET_OK;
+  /* a new plan is built on the host from the activity map and uploaded */
   const size_t nv = sc->activity.size();
   const double T = (double)sc->cfg.acquisition_time_ps * 1e-12;
   std::vector<Emitter> em;
@@ -256,6 +260,7 @@ mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
     d.emitters_cap = cap;
   }
   if (!em.empty()) CUDA_TRY(cudaMemcpy(d.emitters, em.data(), em.size() * sizeof(Emitter), cudaMemcpyHostToDevice));
+  d.run_h2d += (long long)(em.size() * sizeof(Emitter));
   d.n_emitters = (int)em.size();
   d.n_lanes = lanes;
   d.plan_key = key;
@@ -283,6 +288,7 @@ int auto_hpl(const mcpet_scene* sc) {
 /* Enqueue one transport run writing into the device tallies O. */
 mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTallies O, cudaStream_t st,
                          double* ms_out) {
+  sc->dev.run_h2d = 0;
   mcpet_status s = ensure_device(sc);
   if (s != MCPET_OK) return s;
   s = upload_tables(sc);
@@ -323,6 +329,8 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   if (O.spectrum) CUDA_TRY(cudaMemsetAsync(O.spectrum, 0, (size_t)sc->cfg.n_energy_bins * 4, st));
   CUDA_TRY(cudaMemsetAsync(O.psf_count, 0, 4, st));
   CUDA_TRY(cudaMemsetAsync(O.histories, 0, 8, st));
+  if (!O.coincidences) O.coincidences = small + 14;
+  CUDA_TRY(cudaMemsetAsync(O.coincidences, 0, 8, st));
   if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
   if (!sino) {
     /* the kernel only touches the spectrum when the sinogram is tallied */
@@ -340,6 +348,7 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   int grid = d.sm_count * bps;
+  d.last_h2d = d.run_h2d + (long long)sizeof(TransportParams);
   if (P.n_lanes == 0) grid = 1;
   if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
   CUDA_TRY(launch_transport(P, device_tables(sc), O, counters, grid, block, smem, st));
@@ -509,6 +518,9 @@ mcpet_status mcpet_scene_get_info(const mcpet_scene* sc, mcpet_scene_info* info)
   info->n_palette = (int)sc->palette.size();
   info->n_bins = sc->cfg.n_bins;
   info->n_energy_spectrum = sc->cfg.n_energy_bins;
+  info->n_emitters = sc->dev.n_emitters;
+  info->n_lanes = (long long)sc->dev.n_lanes;
+  info->last_h2d_bytes = sc->dev.last_h2d;
   return MCPET_OK;
 }
 
@@ -568,6 +580,7 @@ mcpet_status mcpet_run_device(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet
   O.psf = (uint32_t*)out->psf;
   O.psf_count = out->psf_count;
   O.histories = out->total_histories;
+  O.coincidences = out->coincidences;
   O.counters = (unsigned long long*)out->counters;
   cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
   double ms = 0;
@@ -596,6 +609,7 @@ mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallie
   O.psf = want_psf ? d.psf : nullptr;
   O.histories = d.small + 2;
   O.psf_count = (int*)(d.small + 3);
+  O.coincidences = d.small + 14;
   O.counters = (opts && opts->collect_counters) ? d.small + 4 : nullptr;
   cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
   double ms = 0;
@@ -616,6 +630,7 @@ mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallie
   int psf_count = (int)(small[3] & 0xffffffffull);
   if (out->psf_count) *out->psf_count = psf_count;
   if (out->total_histories) *out->total_histories = small[2];
+  if (out->coincidences) *out->coincidences = small[14];
   if (want_psf) {
     long long n = std::min<long long>(std::max(psf_count, 0), std::min<long long>(d.psf_cap, out->psf_capacity));
     if (n > 0) CUDA_TRY(cudaMemcpy(out->psf, d.psf, (size_t)n * 44, cudaMemcpyDeviceToHost));

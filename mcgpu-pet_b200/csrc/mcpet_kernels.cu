@@ -190,7 +190,8 @@ __device__ __forceinline__ void put_psf_record(uint32_t* psf, long long k, unsig
 template <bool kCount>
 __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, const DeviceTallies& O,
                                             int* spec_sh, int voxel, unsigned long long t_left,
-                                            const PhotonState& b, const PhotonState& a, LaneCounters& cnt) {
+                                            const PhotonState& b, const PhotonState& a, LaneCounters& cnt,
+                                            unsigned long long& detected) {
   const bool want_sino = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 2);
   const bool want_psf = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 1);
   if (want_sino) {
@@ -228,6 +229,7 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
                 atomicAdd(&O.scatter[bin], 1);
                 atomicAdd(&O.image_scatter[voxel], 1);
               }
+              detected += 1;
               Counting<kCount>::add(cnt.tallies, 2);
             } else {
               Counting<true>::add(cnt.guard, 1);
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
   __syncthreads();
 
   LaneCounters cnt = {};
-  unsigned long long histories = 0;
+  unsigned long long histories = 0, detected = 0;
   const bool background = P.background_mode != 0;
   for (;;) {
     uint64_t lane = claim_lane(O.lane_cursor);
@@ -345,12 +347,13 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       if (esc_a && esc_b) {
         bool pass = (P.tally_type == 0) || (P.tally_type == 1 && b.state == 0 && a.state == 0) ||
                     (P.tally_type == 2 && (b.state != 0 || a.state != 0));
-        if (pass) detect_pair<kCount>(rng, P, O, spec_sh, voxel, t_left, b, a, cnt);
+        if (pass) detect_pair<kCount>(rng, P, O, spec_sh, voxel, t_left, b, a, cnt, detected);
       }
     }
   }
 
   atomicAdd(O.histories, histories);
+  if (detected) atomicAdd(O.coincidences, detected);
   if (cnt.guard) atomicAdd(O.guard, cnt.guard);
   if (kCount && O.counters) {
     atomicAdd(&O.counters[0], cnt.steps);

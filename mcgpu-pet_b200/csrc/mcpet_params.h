@@ -115,6 +115,7 @@ struct DeviceTallies {
   uint32_t* psf;                  /* 11 words per packed 44-byte record */
   int* psf_count;
   unsigned long long* histories;
+  unsigned long long* coincidences;
   unsigned long long* counters;   /* 10 counters (mcpet_counters order) or NULL */
   unsigned long long* guard;      /* guard trips */
   unsigned long long* lane_cursor;/* lane work queue head */

@@ -70,6 +70,8 @@ struct mcpet_scene {
     void* ev0 = nullptr;
     void* ev1 = nullptr;
     unsigned long long last_guard = 0;
+    long long run_h2d = 0;        /* host->device bytes of the run in progress */
+    long long last_h2d = 0;       /* ... and of the last completed run */
   } dev;
 
   ~mcpet_scene();

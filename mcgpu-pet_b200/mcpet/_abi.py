@@ -94,6 +94,9 @@ class SceneInfo(C.Structure):
         ("density_nominal", C.c_float * MAX_MATERIALS),
         ("n_bins", C.c_longlong),
         ("n_energy_spectrum", C.c_int),
+        ("n_emitters", C.c_int),
+        ("n_lanes", C.c_longlong),
+        ("last_h2d_bytes", C.c_longlong),
     ]
 
 
@@ -136,6 +139,7 @@ class Tallies(C.Structure):
         ("psf_capacity", C.c_longlong),
         ("psf_count", C.c_void_p),
         ("total_histories", C.c_void_p),
+        ("coincidences", C.c_void_p),
         ("counters", C.c_void_p),
         ("transport_ms", C.c_void_p),
     ]

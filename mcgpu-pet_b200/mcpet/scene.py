@@ -62,6 +62,7 @@ class RunResult:
     total_histories: int
     transport_ms: float
     counters: dict = field(default_factory=dict)
+    detected: int = 0                  # coincidences counted by the kernel
 
     @property
     def coincidences(self) -> int:
@@ -207,6 +208,7 @@ class Scene:
         psf = np.zeros(cap, PSF_DTYPE) if cap > 0 else None
         psf_count = C.c_int32(0)
         hist = C.c_ulonglong(0)
+        det = C.c_ulonglong(0)
         ms = C.c_double(0)
         cnt = _abi.Counters()
         t = _abi.Tallies()
@@ -216,6 +218,7 @@ class Scene:
         t.psf_capacity = cap
         t.psf_count = C.addressof(psf_count)
         t.total_histories = C.addressof(hist)
+        t.coincidences = C.addressof(det)
         t.counters = C.addressof(cnt)
         t.transport_ms = C.addressof(ms)
         co = opts.to_c()
@@ -224,7 +227,39 @@ class Scene:
         counters = {name: int(getattr(cnt, name)) for name, _ in _abi.Counters._fields_}
         return RunResult(trues, scatter, img_t, img_s, spec,
                          psf[: max(0, min(n, cap))] if psf is not None else None, n, int(hist.value),
-                         float(ms.value), counters)
+                         float(ms.value), counters, int(det.value))
+
+    def run_into(self, host: dict, opts: Optional[RunOptions] = None) -> dict:
+        """End-to-end run (mcpet_run) writing into caller-provided host buffers
+        (numpy arrays or pinned torch CPU tensors): trues, scatter,
+        image_trues, image_scatter, spectrum.  Returns the scalar results."""
+        opts = opts or RunOptions()
+
+        def p(name):
+            x = host.get(name)
+            if x is None:
+                return None
+            return x.data_ptr() if hasattr(x, "data_ptr") else _ptr(x)
+
+        psf_count = C.c_int32(0)
+        hist = C.c_ulonglong(0)
+        det = C.c_ulonglong(0)
+        ms = C.c_double(0)
+        t = _abi.Tallies()
+        t.trues, t.scatter = p("trues"), p("scatter")
+        t.image_trues, t.image_scatter = p("image_trues"), p("image_scatter")
+        t.spectrum = p("spectrum")
+        t.psf_count = C.addressof(psf_count)
+        t.total_histories = C.addressof(hist)
+        t.coincidences = C.addressof(det)
+        t.transport_ms = C.addressof(ms)
+        co = opts.to_c()
+        check(lib().mcpet_run(self._h, C.byref(co), C.byref(t)))
+        return {"coincidences": int(det.value), "total_histories": int(hist.value), "transport_ms": ms.value,
+                "psf_count": psf_count.value}
+
+    def last_upload_bytes(self) -> int:
+        return int(self.info.last_h2d_bytes)
 
     def run_device(self, tallies: dict, opts: Optional[RunOptions] = None, time_it: bool = False) -> float:
         """Run into caller-owned torch CUDA tensors (mcpet_run_device).
@@ -248,6 +283,7 @@ class Scene:
         t.psf_capacity = 0 if tallies.get("psf") is None else tallies["psf"].numel() // _abi.PSF_RECORD_BYTES
         t.psf_count = p("psf_count")
         t.total_histories = p("histories")
+        t.coincidences = p("coincidences")
         t.counters = p("counters")
         t.transport_ms = C.addressof(ms) if time_it else None
         co = opts.to_c()

@@ -4,12 +4,8 @@
  * oracle/_ref/libref_cuda.so from the reference sources where they lie
  * (MCGPU-PET.cu, which #includes MCGPU-PET.h and MCGPU-PET_kernel.cu), with
  * the reference's own flags (-DUSING_CUDA -O3 -use_fast_math, Makefile:44)
- * retargeted to sm_100a.  Two groups of entry points:
+ * retargeted to sm_100a:
  *
- *   refio_*  host-only: the reference's input parser and loaders
- *            (read_input MCGPU-PET.cu:866, load_voxels :1381,
- *            load_material :1565), used to pin the product's parser and
- *            table builder bit for bit.  These never touch the GPU.
  *   refh_*   GPU harnesses that run the reference's device functions
  *            (init_PRNG/ranecu, source, GCOa, GRAa, tally_Sinogram) on a
  *            B200 so the product's kernels can be compared bit for bit on
@@ -47,9 +43,9 @@ __device__ unsigned long long capture_atomic_add(unsigned long long* p, unsigned
 #include <string.h>
 #include <unistd.h>
 
-/* ------------------------------------------------------------------ refio */
+/* Parameter block of the harnesses (same leading layout as refc_params in
+ * ref_cpu.cpp and refio_config in ref_prog.cu). */
 extern "C" {
-
 typedef struct {
   int nx, ny, nz;
   float inv_vx, inv_vy, inv_vz;
@@ -63,126 +59,8 @@ typedef struct {
   float e_resol, e_low, e_high, fovz;
   int nrows, ncrystals, nangles, nrad, nzs, nbins, res, nvoxs, ne, mrd, span, nsinos;
   int tpb, seed, peta;
-  /* extra parse results */
-  int gpu_id, nseg, flag_material_dose;
-  float fact_object;
-  short roi[6];
-  float activity[MAX_MATERIALS];
-  float density_max[MAX_MATERIALS];
-  float density_nominal[MAX_MATERIALS];
-  char voxel_file[250];
-  char psf_file[250];
-  char dose_file[250];
-  char materials[MAX_MATERIALS][250];
-} refio_config;
-
-typedef struct {
-  refio_config cfg;
-  float3* voxels;
-  float2* woodcock;
-  float3* a;
-  float3* b;
-  compton_struct* cmp;
-  rayleigh_struct* ray;
-  PSF_element_struct* psf;
-} refio_handle;
-
-/* Parse the input file and load phantom + materials exactly as the reference
- * main() does up to the detector auto-centring (MCGPU-PET.cu:228-322).
- * Relative file names resolve against the current directory, as in the
- * reference.  The reference exit()s on malformed input. */
-void* refio_open(const char* in_path) {
-  refio_handle* h = (refio_handle*)calloc(1, sizeof(refio_handle));
-  h->cmp = (compton_struct*)calloc(1, sizeof(compton_struct));
-  h->ray = (rayleigh_struct*)calloc(1, sizeof(rayleigh_struct));
-  refio_config* c = &h->cfg;
-  char arg0[] = "ref", arg1[1024];
-  strncpy(arg1, in_path, sizeof(arg1) - 1);
-  char* argv[] = {arg0, arg1, nullptr};
-  unsigned long long total_histories = 0, psf_bytes = 0;
-  int hpt = 0, num_projections = 1, voxels_Edep_bytes = 0;
-  detector_struct det; source_struct src; source_energy_struct srce;
-  memset(&det, 0, sizeof(det)); memset(&src, 0, sizeof(src)); memset(&srce, 0, sizeof(srce));
-  char espc[250];
-  double D_angle = -1.0, a0 = 0.0, a1 = 360.0, ia = 0.0, srad = -1.0, vt = 0.0;
-  ulonglong2* vedep = nullptr;
-  read_input(2, argv, 0, &total_histories, &c->seed, &c->gpu_id, &c->tpb, &hpt, &det, &h->psf,
-             &psf_bytes, &src, &srce, c->voxel_file, c->materials, c->psf_file, espc,
-             &num_projections, &D_angle, &a0, &a1, &ia, &vedep, &voxels_Edep_bytes, c->dose_file,
-             &c->roi[0], &c->roi[1], &c->roi[2], &c->roi[3], &c->roi[4], &c->roi[5], &srad, &vt,
-             &c->flag_material_dose, &c->fact_object, &c->e_resol, &c->e_low, &c->e_high, &c->fovz,
-             &c->nrows, &c->ncrystals, &c->nangles, &c->nrad, &c->nzs, &c->nbins, &c->res,
-             &c->nvoxs, &c->ne, &c->mrd, &c->span, &c->nseg, &c->nsinos);
-  free(vedep);
-  voxel_struct vd;
-  unsigned int vbytes = 0;
-  load_voxels(0, c->voxel_file, c->density_max, &c->fact_object, &vd, &h->voxels, &vbytes,
-              &c->roi[1], &c->roi[3], &c->roi[5]);
-  linear_interp lin;
-  int wbytes = 0, tbytes = 0;
-  load_material(0, c->materials, c->density_max, c->density_nominal, &lin, &h->woodcock, &wbytes,
-                &h->a, &h->b, &tbytes, h->ray, h->cmp);
-  if (det.PSF_radius < 0.0f) {   /* auto-centring performed by main(), MCGPU-PET.cu:316-322 */
-    det.PSF_center.x = vd.size_bbox.x * 0.5f;
-    det.PSF_center.y = vd.size_bbox.y * 0.5f;
-    det.PSF_center.z = vd.size_bbox.z * 0.5f;
-    det.PSF_radius = -det.PSF_radius;
-  }
-  c->nx = vd.num_voxels.x; c->ny = vd.num_voxels.y; c->nz = vd.num_voxels.z;
-  c->inv_vx = vd.inv_voxel_size.x; c->inv_vy = vd.inv_voxel_size.y; c->inv_vz = vd.inv_voxel_size.z;
-  c->bbx = vd.size_bbox.x; c->bby = vd.size_bbox.y; c->bbz = vd.size_bbox.z;
-  c->n_e = lin.num_values; c->e0 = lin.e0; c->ide = lin.ide;
-  c->cx = det.PSF_center.x; c->cy = det.PSF_center.y; c->cz = det.PSF_center.z;
-  c->radius = det.PSF_radius; c->height = det.PSF_height; c->psf_size = det.PSF_size;
-  c->tally_psf_sino = det.tally_PSF_SINOGRAM; c->tally_type = det.tally_TYPE;
-  c->acq_ps = src.acquisition_time_ps; c->mean_life = src.mean_life;
-  memcpy(c->activity, src.activity, sizeof(c->activity));
-  c->peta = 1;
-  return h;
+} refh_params;
 }
-
-void refio_get_config(void* hp, refio_config* out) { *out = ((refio_handle*)hp)->cfg; }
-int refio_sizeof_config(void) { return (int)sizeof(refio_config); }
-
-void refio_get_voxels(void* hp, float* out) {
-  refio_handle* h = (refio_handle*)hp;
-  memcpy(out, h->voxels, sizeof(float3) * (size_t)h->cfg.nx * h->cfg.ny * h->cfg.nz);
-}
-
-/* woodcock: float2[n_e]; a,b: float3[n_e*15]; then the flat Compton/Rayleigh arrays. */
-void refio_get_tables(void* hp, float* woodcock, float* a, float* b, float* fco, float* uico,
-                      float* fj0, int* noscco, float* xco, float* pco, float* aco, float* bco,
-                      float* pmax, unsigned char* itlco, unsigned char* ituco) {
-  refio_handle* h = (refio_handle*)hp;
-  size_t ne = (size_t)h->cfg.n_e;
-  memcpy(woodcock, h->woodcock, sizeof(float2) * ne);
-  memcpy(a, h->a, sizeof(float3) * ne * MAX_MATERIALS);
-  memcpy(b, h->b, sizeof(float3) * ne * MAX_MATERIALS);
-  memcpy(fco, h->cmp->fco, sizeof(h->cmp->fco));
-  memcpy(uico, h->cmp->uico, sizeof(h->cmp->uico));
-  memcpy(fj0, h->cmp->fj0, sizeof(h->cmp->fj0));
-  memcpy(noscco, h->cmp->noscco, sizeof(h->cmp->noscco));
-  memcpy(xco, h->ray->xco, sizeof(h->ray->xco));
-  memcpy(pco, h->ray->pco, sizeof(h->ray->pco));
-  memcpy(aco, h->ray->aco, sizeof(h->ray->aco));
-  memcpy(bco, h->ray->bco, sizeof(h->ray->bco));
-  memcpy(pmax, h->ray->pmax, sizeof(h->ray->pmax));
-  memcpy(itlco, h->ray->itlco, sizeof(h->ray->itlco));
-  memcpy(ituco, h->ray->ituco, sizeof(h->ray->ituco));
-}
-
-void refio_close(void* hp) {
-  refio_handle* h = (refio_handle*)hp;
-  if (!h) return;
-  free(h->voxels); free(h->woodcock); free(h->a); free(h->b); free(h->psf);
-  free(h->cmp); free(h->ray); free(h);
-}
-
-/* NSINOS/NSEG/NBINS exactly as read_input computes them (MCGPU-PET.cu:1176-1189),
- * by parsing a minimal input that only differs in the sinogram section is
- * unnecessary: the formula is exposed through refio_open's config. */
-
-}  /* extern "C" */
 
 /* ------------------------------------------------------------------ refh */
 #define HCHK(x)                                                                        \
@@ -293,7 +171,7 @@ int refh_prng(int n, int seed_input, const int* tids, int ndraw, int* seeds_out,
 }
 
 /* Same outputs as refc_sinogram_events in ref_cpu.cpp (6 ints per event). */
-int refh_sinogram_events(const refio_config* p, int n, const float* e2, const float* e1,
+int refh_sinogram_events(const refh_params* p, int n, const float* e2, const float* e1,
                          const float* pos2, const float* pos1, const float* dir2,
                          const float* dir1, const signed char* st2, const signed char* st1,
                          const int* seeds, int* out) {

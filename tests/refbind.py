@@ -1,6 +1,8 @@
 """Bindings of the reference builds under oracle/_ref (test infrastructure).
 
-* ``RefIO``   -- the reference parser/loaders (host code of libref_cuda.so);
+* ``RefIO``   -- the reference parser/loaders (host code of libref_prog.so);
+* ``RefProg`` -- the reference transport run as its main() performs it, with
+                 the kernel timed by CUDA events (libref_prog.so, needs a GPU);
 * ``RefGPU``  -- GPU harnesses running the reference's own device functions
                  (libref_cuda.so, needs a GPU);
 * ``RefCPU``  -- the reference transport kernel compiled for the host
@@ -138,7 +140,7 @@ class RefIO:
     """read_input + load_voxels + load_material of the reference (host only)."""
 
     def __init__(self):
-        self.L = C.CDLL(os.path.join(REF_DIR, "libref_cuda.so"))
+        self.L = C.CDLL(os.path.join(REF_DIR, "libref_prog.so"))
         self.L.refio_open.restype = P
         self.L.refio_open.argtypes = [C.c_char_p]
         for n in ["refio_get_config", "refio_get_voxels", "refio_close"]:
@@ -197,7 +199,7 @@ class RefCPU:
         self.L.refc_run.argtypes = [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, C.c_longlong, C.c_int]
         self.L.refc_run.restype = C.c_int
         self.L.refc_prng.argtypes = [C.c_int, C.c_int, P, C.c_int, P, P, P]
-        self.L.refc_sinogram_events.argtypes = [P, C.c_int] + [P] * 14
+        self.L.refc_sinogram_events.argtypes = [P, C.c_int] + [P] * 15
         self.L.refc_gcoa.argtypes = [C.c_int, P, P, P, P, P, P, P]
         self.L.refc_graa.argtypes = [C.c_int, P, P, P, P, P, P, P]
         self.L.refc_abmodm.argtypes = [C.c_int, C.c_int, C.c_int]
@@ -285,6 +287,45 @@ def _event_arrays(ev: dict) -> dict:
             for k in ["e2", "e1", "pos2", "pos1", "dir2", "dir1", "st2", "st1", "seeds"]}
 
 
+class ProgOutputs(C.Structure):
+    _fields_ = [("trues", P), ("scatter", P), ("image_trues", P), ("image_scatter", P), ("spectrum", P),
+                ("psf", P), ("psf_capacity", C.c_longlong), ("psf_count", C.c_int),
+                ("total_histories", C.c_ulonglong), ("kernel_ms", C.c_float), ("nbins", C.c_int),
+                ("nvox", C.c_int), ("ne", C.c_int)]
+
+
+class RefProg:
+    """The reference's own transport run (read_input .. track_particles) on the GPU."""
+
+    def __init__(self):
+        self.L = C.CDLL(os.path.join(REF_DIR, "libref_prog.so"))
+        self.L.refp_run.argtypes = [C.c_char_p, C.c_int, P]
+        self.L.refp_run.restype = C.c_int
+
+    def run(self, in_path: str, nbins: int, nvox: int, ne: int, background: bool = False, psf_capacity: int = 0,
+            cwd: Optional[str] = None) -> dict:
+        out = {"trues": np.zeros(nbins, np.int32), "scatter": np.zeros(nbins, np.int32),
+               "image_trues": np.zeros(nvox, np.int32), "image_scatter": np.zeros(nvox, np.int32),
+               "spectrum": np.zeros(max(ne, 1), np.int32)}
+        psf = np.zeros(max(psf_capacity, 1) * 44, np.uint8)
+        o = ProgOutputs()
+        for k in ["trues", "scatter", "image_trues", "image_scatter", "spectrum"]:
+            setattr(o, k, _p(out[k]))
+        o.psf = _p(psf)
+        o.psf_capacity = psf_capacity
+        with _chdir(cwd):
+            rc = _quiet_call(self.L.refp_run, os.fsencode(in_path), int(bool(background)), C.byref(o))
+        if rc != 0:
+            raise RuntimeError(f"reference run failed with CUDA error {rc}")
+        assert (o.nbins, o.nvox) == (nbins, nvox)
+        out["psf_count"] = o.psf_count
+        out["total_histories"] = int(o.total_histories)
+        out["kernel_ms"] = float(o.kernel_ms)
+        n = max(0, min(o.psf_count, psf_capacity))
+        out["psf_raw"] = psf[: n * 44]
+        return out
+
+
 class RefGPU:
     """Reference device functions on the GPU (libref_cuda.so harnesses)."""
 
@@ -309,12 +350,10 @@ class RefGPU:
         return s, f, d
 
     def sinogram_events(self, p: Params, ev: dict) -> np.ndarray:
-        cfg = IOConfig()
-        C.memmove(C.addressof(cfg), C.addressof(p), C.sizeof(Params))
         n = len(ev["e2"])
         a = _event_arrays(ev)
         out = np.zeros((n, 6), np.int32)
-        assert self.L.refh_sinogram_events(C.byref(cfg), n, _p(a["e2"]), _p(a["e1"]), _p(a["pos2"]),
+        assert self.L.refh_sinogram_events(C.byref(p), n, _p(a["e2"]), _p(a["e1"]), _p(a["pos2"]),
                                            _p(a["pos1"]), _p(a["dir2"]), _p(a["dir1"]), _p(a["st2"]),
                                            _p(a["st1"]), _p(a["seeds"]), _p(out)) == 0
         return out

@@ -55,11 +55,19 @@ def random_events(n: int, rng: np.random.Generator, box=(9.0, 9.0, 9.0), seeds=N
     if seeds is None:
         seeds = np.stack([rng.integers(1, 2147483562, n), rng.integers(1, 2147483398, n)], 1).astype(np.int32)
     b = np.asarray(box, np.float32)
+    d1 = dirs(n)
+    # half of the pairs nearly back to back (as annihilation photons), half independent
+    d2 = dirs(n)
+    k = n // 2
+    jitter = -d1[:k].astype(np.float64) + rng.normal(0, 0.02, (k, 3))
+    d2[:k] = (jitter / np.linalg.norm(jitter, axis=1, keepdims=True)).astype(np.float32)
+    p1 = (rng.uniform(0, 1, (n, 3)) * b).astype(np.float32)
+    p2 = (rng.uniform(0, 1, (n, 3)) * b).astype(np.float32)
+    p2[:k] = p1[:k]
     return dict(
         e2=rng.uniform(*e_range, n).astype(np.float32), e1=rng.uniform(*e_range, n).astype(np.float32),
-        pos2=(rng.uniform(0, 1, (n, 3)) * b).astype(np.float32), pos1=(rng.uniform(0, 1, (n, 3)) * b).astype(np.float32),
-        dir2=dirs(n), dir1=dirs(n), st2=rng.integers(0, 4, n).astype(np.int8), st1=rng.integers(0, 4, n).astype(np.int8),
-        seeds=seeds.astype(np.int32),
+        pos2=p2, pos1=p1, dir2=d2, dir1=d1, st2=rng.integers(0, 4, n).astype(np.int8),
+        st1=rng.integers(0, 4, n).astype(np.int8), seeds=seeds.astype(np.int32),
     )
 
 
