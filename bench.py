@@ -55,11 +55,17 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def build_workload(workdir: str, emissions: float):
+def build_workload(workdir: str, emissions: float, scanner: str = "head"):
     from mcpet import inputs
     mat, rho, act, vs, used = inputs.head_phantom(shape=(64, 128, 128), voxel_cm=0.2, seed=PHANTOM_SEED,
                                                   total_bq=emissions)
-    spec = inputs.spec_for(inputs.tissue_materials(used), "unused.vox", seed=12345, **inputs.scanner_for_head())
+    scan = inputs.scanner_for_head()
+    if scanner == "head32":
+        # profiling variant: same phantom and ring pitch, 32 rings, 128x128 bins
+        # (2 x 130 MB of sinograms instead of 2 x 2.1 GB)
+        scan.update(n_rows=32, n_z_slices=63, max_ring_difference=31, n_radial=128, n_angles=256, n_crystals=512,
+                    fov_z=12.8, detector_height=12.8)
+    spec = inputs.spec_for(inputs.tissue_materials(used), "unused.vox", seed=12345, **scan)
     cfg = inputs.config_from_spec(spec, workdir)
     return cfg, mat, rho, act, vs
 
@@ -198,6 +204,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scanner", default="head", choices=["head", "head32"],
+                    help="head32: smaller sinogram for profiler captures (not a bench line)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -219,7 +227,7 @@ def main():
     lanes = mcpet.LANES_BALANCED if args.lanes == "balanced" else mcpet.LANES_REFERENCE
 
     tmp = tempfile.mkdtemp()
-    cfg, mat, rho, act, vs = build_workload(tmp, args.emissions)
+    cfg, mat, rho, act, vs = build_workload(tmp, args.emissions, args.scanner)
     scene = mcpet.Scene.from_arrays(cfg, mat, rho, act, vs)
     scene.to_device(local)
     nb, nv, ne = int(cfg.n_bins), int(scene.info.n_voxels), cfg.n_energy_bins

@@ -285,11 +285,21 @@ int auto_hpl(const mcpet_scene* sc) {
   return (int)h;
 }
 
+mcpet_status validate_opts(const mcpet_scene* sc, const mcpet_run_opts* opts) {
+  int seed = (opts && opts->seed_override != 0) ? opts->seed_override : sc->cfg.seed;
+  if (seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", seed);
+  if (opts && (opts->lane_mode < 0 || opts->lane_mode > 1))
+    return set_error(MCPET_ERR_ARG, "unknown lane mode %d", opts->lane_mode);
+  return MCPET_OK;
+}
+
 /* Enqueue one transport run writing into the device tallies O. */
 mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTallies O, cudaStream_t st,
                          double* ms_out) {
   sc->dev.run_h2d = 0;
-  mcpet_status s = ensure_device(sc);
+  mcpet_status s = validate_opts(sc, opts);
+  if (s != MCPET_OK) return s;
+  s = ensure_device(sc);
   if (s != MCPET_OK) return s;
   s = upload_tables(sc);
   if (s != MCPET_OK) return s;
@@ -591,7 +601,9 @@ mcpet_status mcpet_run_device(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet
 
 mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out) {
   if (!sc || !out) return set_error(MCPET_ERR_ARG, "null argument");
-  mcpet_status s = ensure_device(sc);
+  mcpet_status s = validate_opts(sc, opts);
+  if (s != MCPET_OK) return s;
+  s = ensure_device(sc);
   if (s != MCPET_OK) return s;
   s = upload_tables(sc);
   if (s != MCPET_OK) return s;

@@ -127,15 +127,20 @@ def test_statistics_vs_oracle_water_cube(workdir, lane_mode):
 
 
 def test_statistics_vs_oracle_head(workdir):
-    sc = scenes.small_head_scene(workdir, total_bq=6.0e5, shape=(24, 48, 48), voxel_cm=0.5)
+    sc = scenes.small_head_scene(workdir, total_bq=2.0e6, shape=(24, 48, 48), voxel_cm=0.5)
     res, ref = _oracle_pair(sc, 77, 78, mcpet.LANES_BALANCED)
     cfg = sc.config
     for k in ("trues", "scatter"):
         a, b = int(getattr(res, k).sum()), int(ref[k].sum())
         assert abs(a - b) <= 3 * math.sqrt(a + b) + 1, (k, a, b)
-    chi, dof = scenes.chi2_per_dof(coarse(res.trues + res.scatter, cfg, (64, 16, 16)),
-                                   coarse(ref["trues"] + ref["scatter"], cfg, (64, 16, 16)), min_count=20)
-    assert dof > 500 and 0.85 <= chi <= 1.15, (chi, dof)
+    # 8065 x 256 x 256 sinogram -> 8 x 16 x 32 coarse bins
+    f = (1009, 16, 8)
+    chi, dof = scenes.chi2_per_dof(coarse(res.trues + res.scatter, cfg, f), coarse(ref["trues"] + ref["scatter"],
+                                                                                   cfg, f), min_count=20)
+    assert dof > 800 and 0.9 <= chi <= 1.1, (chi, dof)
+    chi, dof = scenes.chi2_per_dof(res.image_trues + res.image_scatter, ref["image_trues"] + ref["image_scatter"],
+                                   min_count=20)
+    assert dof > 200 and 0.8 <= chi <= 1.2, (chi, dof)
     sc.close()
 
 
