@@ -204,6 +204,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--algorithm", default="auto", choices=["auto", "histories", "events"])
     ap.add_argument("--scanner", default="head", choices=["head", "head32"],
                     help="head32: smaller sinogram for profiler captures (not a bench line)")
     args = ap.parse_args()
@@ -245,9 +246,12 @@ def main():
     stream = torch.cuda.current_stream(dev)
     base_seed = 12345 + 7919 * rank
 
+    algorithm = {"auto": mcpet.ALGORITHM_AUTO, "histories": mcpet.ALGORITHM_HISTORIES,
+                 "events": mcpet.ALGORITHM_EVENTS}[args.algorithm]
+
     def opts(step, counters=False):
         return mcpet.RunOptions(lane_mode=lanes, seed_override=base_seed + step, collect_counters=counters,
-                                stream=stream.cuda_stream)
+                                stream=stream.cuda_stream, algorithm=algorithm)
 
     # algorithmic-byte counters of one launch (separate, untimed, same seed as step 0)
     scene.run_device(tallies, opts(0, counters=True))
@@ -305,7 +309,8 @@ def main():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             scene.set_activity(act_pinned.numpy())
-            r = scene.run_into(pin, mcpet.RunOptions(lane_mode=lanes, seed_override=base_seed + 500 + k))
+            r = scene.run_into(pin, mcpet.RunOptions(lane_mode=lanes, seed_override=base_seed + 500 + k,
+                                                     algorithm=algorithm))
             dt = time.perf_counter() - t0
             if k > 0:    # first pass warms the host plan builder
                 e2e_coinc += r["coincidences"]
@@ -346,7 +351,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded head phantom, random-free tables from the reference's air/water data)",
                 "config": {"workload": WORKLOAD, "emissions_per_step_per_gpu": args.emissions,
-                           "lanes": args.lanes, "parallelism": f"replicas x{world}",
+                           "lanes": args.lanes, "algorithm": args.algorithm, "parallelism": f"replicas x{world}",
                            "l2": "each step zeroes 4.2 GB of sinograms (> 126 MB L2) before the kernel",
                            "coincidences_per_step": total / args.steps / world, "histories_last_step": hist,
                            "guard_trips": guard},

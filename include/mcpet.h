@@ -126,6 +126,8 @@ typedef struct {
   int collect_counters;           /* 1: also fill mcpet_tallies.counters (slower kernel variant) */
   int seed_override;              /* != 0: use this RANECU seed instead of the scene's */
   void* stream;                   /* cudaStream_t; NULL = default stream */
+  int algorithm;                  /* 0 automatic, 1 history loop per thread, 2 warp-regrouped event loop
+                                     (same results, different schedule) */
 } mcpet_run_opts;
 
 /* Event counters (when collect_counters=1). */

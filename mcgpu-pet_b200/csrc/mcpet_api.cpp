@@ -3,6 +3,7 @@
 #include <cuda_runtime_api.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -73,6 +74,14 @@ int pick_device(int requested) {
   return requested;
 }
 
+/* Tuning knob from the environment, clamped to [lo, hi]. */
+int env_int(const char* name, int def, int lo, int hi) {
+  const char* v = getenv(name);
+  if (!v || !*v) return def;
+  int x = atoi(v);
+  return x < lo ? lo : (x > hi ? hi : x);
+}
+
 void fill_params(const mcpet_scene* sc, TransportParams& P) {
   memset(&P, 0, sizeof(P));
   const mcpet_config& c = sc->cfg;
@@ -121,6 +130,9 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.max_shells = ms;
   P.spectrum_in_shared = (c.n_energy_bins > 0 && c.n_energy_bins <= kSpectrumSharedMax) ? 1 : 0;
   P.palette_in_shared = (sc->palette.size() <= 2048) ? (int)sc->palette.size() : 0;
+  P.e_annihilation = 510998.95f;
+  P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 24, 1, 32);
+  P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 8, 1, 32);
 }
 
 mcpet_status upload_tables(mcpet_scene* sc) {
@@ -290,6 +302,8 @@ mcpet_status validate_opts(const mcpet_scene* sc, const mcpet_run_opts* opts) {
   if (seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", seed);
   if (opts && (opts->lane_mode < 0 || opts->lane_mode > 1))
     return set_error(MCPET_ERR_ARG, "unknown lane mode %d", opts->lane_mode);
+  if (opts && (opts->algorithm < 0 || opts->algorithm > 2))
+    return set_error(MCPET_ERR_ARG, "unknown algorithm %d", opts->algorithm);
   return MCPET_OK;
 }
 
@@ -352,16 +366,18 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   if (block > transport_block_threads()) block = transport_block_threads();
   block = (block / 32) * 32;
   if (block < 32) block = 32;
-  size_t smem = transport_dynamic_smem(P, block);
+  int algorithm = o.algorithm == kAlgorithmHistories ? kAlgorithmHistories : kAlgorithmEvents;
+  if (algorithm == kAlgorithmEvents && env_int("MCPET_DENSE", 0, 0, 1)) algorithm = kAlgorithmEventsDense;
+  size_t smem = transport_dynamic_smem(P, block, algorithm);
   int bps = 0;
-  CUDA_TRY(transport_occupancy(counters, block, smem, &bps));
+  CUDA_TRY(transport_occupancy(counters, algorithm, block, smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   int grid = d.sm_count * bps;
   d.last_h2d = d.run_h2d + (long long)sizeof(TransportParams);
   if (P.n_lanes == 0) grid = 1;
   if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
-  CUDA_TRY(launch_transport(P, device_tables(sc), O, counters, grid, block, smem, st));
+  CUDA_TRY(launch_transport(P, device_tables(sc), O, counters, algorithm, grid, block, smem, st));
   if (ms_out) {
     CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
     CUDA_TRY(cudaEventSynchronize((cudaEvent_t)d.ev1));

@@ -248,18 +248,12 @@ __device__ __forceinline__ bool sample_rayleigh(Rng& r, float energy, int mat, f
  * MCGPU-PET_kernel.cu:1335-1563).  `C` is the block's shared copy of the
  * shell table, `rn` a per-thread scratch of max_shells floats.  Updates the
  * energy; returns false when a rejection guard fired. */
-template <typename Scratch>
-__device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, const ComptonTable& C,
-                                               Scratch rn, double& costh) {
-  const float E = energy;
+/* Incoherent scattering function at theta = pi, the normalisation of the
+ * rejection step of GCOa (MCGPU-PET_kernel.cu:1366-1391).  It depends only on
+ * the energy and material, so kernels evaluate it once per block for the
+ * annihilation energy and pass the value in. */
+__device__ __forceinline__ float compton_s0(float E, int mat, const ComptonTable& C) {
   const int nsh = C.noscco[mat];
-  float ek = E * 1.956951306108245e-6f;
-  float ek2 = ek * 2.f + 1.f;
-  float ek3 = ek * ek;
-  float taumin = 1.f / ek2;
-  float a1 = logf(ek2);
-
-  /* incoherent scattering function at theta = pi */
   float s0 = 0.0f;
   for (int i = 0; i < nsh; ++i) {
     float u = C.uico[mat + i * kMaxMaterials];
@@ -275,6 +269,20 @@ __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, c
       s0 += C.fco[mat + i * kMaxMaterials] * t;
     }
   }
+  return s0;
+}
+
+template <typename Scratch>
+__device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, const ComptonTable& C,
+                                               Scratch rn, double& costh, const float* s0_annihilation = nullptr) {
+  const float E = energy;
+  const int nsh = C.noscco[mat];
+  float ek = E * 1.956951306108245e-6f;
+  float ek2 = ek * 2.f + 1.f;
+  float ek3 = ek * ek;
+  float taumin = 1.f / ek2;
+  float a1 = logf(ek2);
+  const float s0 = (s0_annihilation && E == kAnnihilation) ? s0_annihilation[mat] : compton_s0(E, mat, C);
 
   /* sample tau = E'/E with the Klein-Nishina-like envelope, reject on S */
   float tau, s;

@@ -12,6 +12,8 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+
 #include "mcpet_device.cuh"
 #include "mcpet_kernels.h"
 
@@ -373,6 +375,358 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       if (spec_sh[i]) atomicAdd(&O.spectrum[i], spec_sh[i]);
 }
 
+/* ------------------------------------------------------- event kernel
+ *
+ * transport_events_kernel runs the same per-lane computation as
+ * transport_kernel -- every thread draws the same random numbers and performs
+ * the same floating-point operations for its lane, so the results are
+ * identical -- but schedules it as a state machine regrouped per warp: each
+ * round the warp votes on the phase of its 32 photons and executes ONE phase
+ * for the threads in it.  Woodcock sub-steps (cheap, frequent) run in batches;
+ * Compton sampling (expensive: shell profiles, rejection loops, double
+ * precision rotation) runs only when most of the warp needs it, so its
+ * instructions execute with nearly all lanes active instead of one or two.
+ * Lane-level state that a phase touches once per photon (the pair's emission
+ * point and first photon, the decay clock) lives in shared memory, laid out
+ * [field][thread]. */
+
+enum : int { kPhDecay = 0, kPhStep = 1, kPhCompton = 2, kPhEnd = 3, kPhDone = 4 };  /* kPhCompton: any real scattering */
+
+/* cold per-thread fields in shared memory */
+enum : int {
+  kCOx, kCOy, kCOz, kCDx, kCDy, kCDz,            /* emission point and direction of photon 1 */
+  kCAx, kCAy, kCAz, kCAu, kCAv, kCAw,            /* photon 1 at exit: position, direction */
+  kCAe, kCAt, kCAs,                              /* photon 1 energy (-10 absorbed), travel, state */
+  kCInvLo, kCInvHi, kCTLo, kCTHi, kCVox,         /* lane: 1/rate (double), remaining ps (u64), voxel */
+  kCold
+};
+
+struct ColdState {
+  uint32_t* base;
+  int stride;
+  __device__ __forceinline__ uint32_t& u(int f) const { return base[f * stride]; }
+  __device__ __forceinline__ float f(int k) const { return __uint_as_float(base[k * stride]); }
+  __device__ __forceinline__ void setf(int k, float v) const { base[k * stride] = __float_as_uint(v); }
+  __device__ __forceinline__ double inv_rate() const {
+    return __hiloint2double((int)u(kCInvHi), (int)u(kCInvLo));
+  }
+  __device__ __forceinline__ void set_inv_rate(double v) const {
+    u(kCInvHi) = (uint32_t)__double2hiint(v);
+    u(kCInvLo) = (uint32_t)__double2loint(v);
+  }
+  __device__ __forceinline__ unsigned long long t_left() const {
+    return ((unsigned long long)u(kCTHi) << 32) | u(kCTLo);
+  }
+  __device__ __forceinline__ void set_t_left(unsigned long long v) const {
+    u(kCTHi) = (uint32_t)(v >> 32);
+    u(kCTLo) = (uint32_t)v;
+  }
+};
+
+
+template <bool kCount, int kMinBlocks = 1>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(TransportParams P, DeviceTables T,
+                                                                              DeviceTallies O) {
+  const uint64_t n_lanes = P.n_lanes;
+  const int n_emitters = P.n_emitters;
+  __shared__ ComptonTable cmp;
+  __shared__ float s0_ann[kMaxMaterials];
+  extern __shared__ float4 dyn_smem[];
+  int* spec_sh = nullptr;
+  char* cursor = reinterpret_cast<char*>(dyn_smem);
+  if (P.spectrum_in_shared) {
+    spec_sh = reinterpret_cast<int*>(cursor);
+    cursor += ((P.ne * 4 + 15) / 16) * 16;
+  }
+  const PaletteEntry* pal = T.palette;
+  PaletteEntry* pal_sh = nullptr;
+  if (P.palette_in_shared) {
+    pal_sh = reinterpret_cast<PaletteEntry*>(cursor);
+    cursor += ((P.palette_in_shared * (int)sizeof(PaletteEntry) + 15) / 16) * 16;
+    pal = pal_sh;
+  }
+  SharedScratch rn{reinterpret_cast<float*>(cursor) + threadIdx.x, (int)blockDim.x};
+  cursor += (size_t)(P.max_shells > 0 ? P.max_shells : 1) * blockDim.x * sizeof(float);
+  const ColdState cold{reinterpret_cast<uint32_t*>(cursor) + threadIdx.x, (int)blockDim.x};
+  {
+    const int* src = reinterpret_cast<const int*>(T.compton);
+    int* dst = reinterpret_cast<int*>(&cmp);
+    for (int i = threadIdx.x; i < (int)(sizeof(ComptonTable) / 4); i += blockDim.x) dst[i] = __ldg(&src[i]);
+    if (spec_sh)
+      for (int i = threadIdx.x; i < P.ne; i += blockDim.x) spec_sh[i] = 0;
+    if (pal_sh)
+      for (int i = threadIdx.x; i < P.palette_in_shared; i += blockDim.x) pal_sh[i] = T.palette[i];
+  }
+  __syncthreads();
+  if (threadIdx.x < kMaxMaterials)
+    s0_ann[threadIdx.x] = cmp.noscco[threadIdx.x] > 0 ? compton_s0(P.e_annihilation, threadIdx.x, cmp) : 0.0f;
+  __syncthreads();
+
+  LaneCounters cnt = {};
+  unsigned long long histories = 0, detected = 0;
+  const bool background = P.background_mode != 0;
+  const float2* wood = reinterpret_cast<const float2*>(T.woodcock);
+
+  /* hot per-thread state */
+  Rng rng = {0, 0};
+  int phase = kPhDecay;
+  bool lane_live = false;
+  int which = 1;            /* photon of the pair being tracked */
+  bool fresh = false;       /* next step starts a new interaction-loop iteration */
+  bool escaped = false;
+  bool is_compton = true;   /* pending scattering: Compton (else Rayleigh) */
+  PhotonState ph;
+  ph.pos = make_float3(0.f, 0.f, 0.f);
+  ph.dir = ph.pos;
+  ph.energy = 0.f;
+  ph.travel = 0.f;
+  ph.state = 0;
+  int index = 0, mat_old = -1, mat0 = 0, steps = 0;
+  float mfp_w = 0.f, cax = 0.f, cbx = 0.f;
+  float4 rec_hi = make_float4(0.f, 0.f, 0.f, 0.f);
+
+  /* photon emitted at ph.pos with ph.dir: set up its tracking */
+  auto start_photon = [&]() {
+    ph.energy = kAnnihilation;
+    ph.travel = 0.0f;
+    ph.state = 0;
+    index = __float2int_rd((ph.energy - P.e0) * P.ide);
+    float2 w = __ldg(wood + index);
+    mfp_w = w.x + ph.energy * w.y;
+    mat_old = -1;
+    steps = 0;
+    fresh = true;
+    phase = kPhStep;
+    Counting<kCount>::add(cnt.majorant, 1);
+    Counting<kCount>::add(cnt.photons, 1);
+  };
+
+  for (;;) {
+    const unsigned m_dec = __ballot_sync(0xffffffffu, phase == kPhDecay);
+    const unsigned m_step = __ballot_sync(0xffffffffu, phase == kPhStep);
+    const unsigned m_cmp = __ballot_sync(0xffffffffu, phase == kPhCompton);
+    const unsigned m_end = __ballot_sync(0xffffffffu, phase == kPhEnd);
+    if (!(m_dec | m_step | m_cmp | m_end)) break;
+    /* phase of this round: scattering and pair bookkeeping wait until enough
+     * lanes need them; Woodcock steps fill the rest */
+    const int n_cmp = __popc(m_cmp), n_pair = __popc(m_end | m_dec);
+    int sel;
+    if (n_cmp >= P.quorum_scatter) sel = 0;
+    else if (n_pair >= P.quorum_pair) sel = 1;
+    else if (m_step) sel = 2;
+    else sel = (n_cmp >= n_pair) ? 0 : 1;
+
+    if (sel == 0) {
+      /* ---- real scattering: Compton (MCGPU-PET_kernel.cu:351-373) or
+       * Rayleigh (:375-387), then the common direction update */
+      if (phase == kPhCompton) {
+        double costh = 0.0;
+        bool ok;
+        float e = ph.energy;
+        if (is_compton) {
+          ok = sample_compton(rng, e, mat0, cmp, rn, costh, s0_ann);
+        } else {
+          ok = sample_rayleigh(rng, e, mat0, rec_hi.z, T.rayleigh, costh);
+        }
+        if (!ok) {
+          Counting<true>::add(cnt.guard, 1);
+          escaped = false;
+          phase = kPhEnd;
+        } else {
+          ph.energy = e;
+          rotate(ph.dir, costh, 6.28318530717958647693 * ranecu_double(rng));
+          if (is_compton) {
+            Counting<kCount>::add(cnt.compton, 1);
+            index = __float2int_rd((e - P.e0) * P.ide);
+            if (index > -1) {
+              float2 w = __ldg(wood + index);
+              mfp_w = w.x + e * w.y;
+              mat_old = -2;
+              ph.state = (ph.state == 0) ? 1 : 3;
+              Counting<kCount>::add(cnt.majorant, 1);
+              fresh = true;
+              phase = kPhStep;
+            } else {
+              escaped = false;
+              phase = kPhEnd;
+            }
+          } else {
+            ph.state = (ph.state == 0) ? 2 : 3;
+            Counting<kCount>::add(cnt.rayleigh, 1);
+            fresh = true;
+            phase = kPhStep;
+          }
+        }
+      }
+    } else if (sel == 1) {
+      /* ---- end of a photon: hand over to the second photon, or close the
+       * pair (MCGPU-PET_kernel.cu:417-442); then the next decay */
+      if (phase == kPhEnd) {
+        if (which == 1) {
+          if (escaped) {
+            cold.setf(kCAx, ph.pos.x); cold.setf(kCAy, ph.pos.y); cold.setf(kCAz, ph.pos.z);
+            cold.setf(kCAu, ph.dir.x); cold.setf(kCAv, ph.dir.y); cold.setf(kCAw, ph.dir.z);
+            cold.setf(kCAe, ph.energy); cold.setf(kCAt, ph.travel);
+            cold.u(kCAs) = (uint32_t)ph.state;
+          } else {
+            cold.setf(kCAe, -10.0f);
+          }
+          const float3 d0 = make_float3(cold.f(kCDx), cold.f(kCDy), cold.f(kCDz));
+          emit_second(rng, background, d0, ph.dir);
+          ph.pos = make_float3(cold.f(kCOx), cold.f(kCOy), cold.f(kCOz));
+          which = 2;
+          start_photon();
+        } else {
+          const float ea = cold.f(kCAe);
+          if (escaped && ea > -0.5f) {
+            PhotonState a;
+            a.pos = make_float3(cold.f(kCAx), cold.f(kCAy), cold.f(kCAz));
+            a.dir = make_float3(cold.f(kCAu), cold.f(kCAv), cold.f(kCAw));
+            a.energy = ea;
+            a.travel = cold.f(kCAt);
+            a.state = (int)cold.u(kCAs);
+            const bool pass = (P.tally_type == 0) || (P.tally_type == 1 && ph.state == 0 && a.state == 0) ||
+                              (P.tally_type == 2 && (ph.state != 0 || a.state != 0));
+            if (pass)
+              detect_pair<kCount>(rng, P, O, spec_sh, (int)cold.u(kCVox), cold.t_left(), ph, a, cnt, detected);
+          }
+          phase = kPhDecay;
+        }
+      }
+      /* ---- next decay of the lane, or the next lane (MCGPU-PET_kernel.cu:259-298) */
+      if (phase == kPhDecay) {
+        for (;;) {
+          if (!lane_live) {
+            const uint64_t lane = claim_lane(O.lane_cursor);
+            if (lane >= n_lanes) {
+              phase = kPhDone;
+              break;
+            }
+            const Emitter* em = T.emitters + find_emitter(T.emitters, n_emitters, lane);
+            rng = rng_stream(P, __ldg(&em->stream_base) + (lane - __ldg(&em->first_lane)));
+            cold.set_inv_rate(__ldg(&em->inv_rate));
+            cold.set_t_left(P.acq_ps);
+            cold.u(kCVox) = __ldg(&em->voxel);
+            lane_live = true;
+            Counting<kCount>::add(cnt.lanes, 1);
+          }
+          double inv_act = cold.inv_rate();
+          unsigned long long t_left = cold.t_left();
+          double dt = -log(ranecu_double(rng)) * inv_act;
+          unsigned long long dt_ps = __double2ull_rn(dt * 1e12);
+          if (!(dt_ps < t_left)) {
+            lane_live = false;
+            continue;
+          }
+          cold.set_t_left(t_left - dt_ps);
+          histories += 2;
+          cold.set_inv_rate(inv_act * exp(dt * P.inv_mean_life));
+          const int voxel = (int)cold.u(kCVox);
+          emit_first(rng, P, voxel % P.nx, (voxel / P.nx) % P.ny, voxel / (P.nx * P.ny), ph.pos, ph.dir);
+          cold.setf(kCOx, ph.pos.x); cold.setf(kCOy, ph.pos.y); cold.setf(kCOz, ph.pos.z);
+          cold.setf(kCDx, ph.dir.x); cold.setf(kCDy, ph.dir.y); cold.setf(kCDz, ph.dir.z);
+          which = 1;
+          start_photon();
+          break;
+        }
+      }
+    } else {
+      /* ---- Woodcock sub-steps (MCGPU-PET_kernel.cu:313-393), repeated while
+       * at least half of the warp's stepping photons are still stepping */
+      const int quorum = (__popc(m_step) + 1) >> 1;
+      for (;;) {
+        if (phase == kPhStep) {
+          const float E = ph.energy;
+          bool go = true;
+          if (fresh) {
+            fresh = false;
+            if (locate(P, ph.pos.x, ph.pos.y, ph.pos.z) < 0) {
+              escaped = true;
+              phase = kPhEnd;
+              go = false;
+            }
+          }
+          if (go) {
+            float step = -(mfp_w)*logf(ranecu(rng));
+            ph.travel += step;
+            ph.pos.x += step * ph.dir.x;
+            ph.pos.y += step * ph.dir.y;
+            ph.pos.z += step * ph.dir.z;
+            const int vox = locate(P, ph.pos.x, ph.pos.y, ph.pos.z);
+            if (vox < 0) {
+              escaped = true;
+              phase = kPhEnd;
+            } else if ((unsigned long long)vox >= (unsigned long long)P.n_voxels || ++steps > kMaxWoodcockSteps) {
+              Counting<true>::add(cnt.guard, 1);
+              escaped = false;
+              phase = kPhEnd;
+            } else {
+              const uint32_t key = T.vox16 ? (uint32_t)__ldg(&T.vox16[vox]) : __ldg(&T.vox32[vox]);
+              const PaletteEntry pe = pal[key];
+              mat0 = pe.mat0;
+              Counting<kCount>::add(cnt.steps, 1);
+              const float2* rec = reinterpret_cast<const float2*>(T.mfp + (size_t)index * kMaxMaterials + mat0);
+              if (mat0 != mat_old) {
+                const float2 ab = __ldg(rec);
+                cax = ab.x;
+                cbx = ab.y;
+                mat_old = mat0;
+                Counting<kCount>::add(cnt.refresh, 1);
+              }
+              const float mfp_density = mfp_w * pe.rho;
+              float prob = 1.0f - mfp_density * (cax + E * cbx);
+              const float randno = ranecu(rng);
+              if (!(randno < prob)) {
+                /* real interaction: the record of (energy bin, material) holds
+                 * the same values the reference cached at the last change */
+                const float4 lo = __ldg(reinterpret_cast<const float4*>(rec));
+                rec_hi = __ldg(reinterpret_cast<const float4*>(rec) + 1);
+                prob += mfp_density * (lo.z + E * lo.w);
+                if (randno < prob) {
+                  phase = kPhCompton;
+                  is_compton = true;
+                } else {
+                  prob += mfp_density * (rec_hi.x + E * rec_hi.y);
+                  if (randno < prob) {
+                    phase = kPhCompton;
+                    is_compton = false;
+                  } else {
+                    index = -11;
+                    escaped = false;
+                    phase = kPhEnd;
+                    Counting<kCount>::add(cnt.photo, 1);
+                  }
+                }
+              }
+            }
+          }
+        }
+        if (__popc(__ballot_sync(0xffffffffu, phase == kPhStep)) < quorum) break;
+      }
+    }
+  }
+
+  atomicAdd(O.histories, histories);
+  if (detected) atomicAdd(O.coincidences, detected);
+  if (cnt.guard) atomicAdd(O.guard, cnt.guard);
+  if (kCount && O.counters) {
+    atomicAdd(&O.counters[0], cnt.steps);
+    atomicAdd(&O.counters[1], cnt.refresh);
+    atomicAdd(&O.counters[2], cnt.majorant);
+    atomicAdd(&O.counters[3], cnt.tallies);
+    atomicAdd(&O.counters[4], cnt.photons);
+    atomicAdd(&O.counters[5], cnt.compton);
+    atomicAdd(&O.counters[6], cnt.rayleigh);
+    atomicAdd(&O.counters[7], cnt.photo);
+    atomicAdd(&O.counters[8], cnt.lanes);
+    atomicAdd(&O.counters[9], cnt.guard);
+  }
+  __syncthreads();
+  if (spec_sh)
+    for (int i = threadIdx.x; i < P.ne; i += blockDim.x)
+      if (spec_sh[i]) atomicAdd(&O.spectrum[i], spec_sh[i]);
+}
+
 /* ---------------------------------------------------------- probes */
 
 __global__ void probe_rng_kernel(TransportParams P, int n, const int64_t* ids, int ndraw, int2* seeds,
@@ -485,35 +839,61 @@ __global__ void probe_source_kernel(TransportParams P, int background, int2* see
 
 /* ---------------------------------------------------------- launchers */
 
-size_t transport_dynamic_smem(const TransportParams& P, int block) {
+size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm) {
   size_t s = 0;
   if (P.spectrum_in_shared) s += ((size_t)P.ne * 4 + 15) / 16 * 16;
   if (P.palette_in_shared) s += ((size_t)P.palette_in_shared * sizeof(PaletteEntry) + 15) / 16 * 16;
   s += (size_t)(P.max_shells > 0 ? P.max_shells : 1) * block * sizeof(float);
+  if (algorithm != kAlgorithmHistories) s += (size_t)kCold * block * sizeof(uint32_t);
   return s;
 }
 
 int transport_block_threads() { return kBlock; }
 
-cudaError_t transport_occupancy(bool counters, int block, size_t smem, int* blocks_per_sm) {
-  if (counters)
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<true>, block, smem);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel<false>, block, smem);
+template <typename K>
+static cudaError_t occupancy_smem_attr(K kernel, size_t smem) {
+  /* prefer shared memory over L1 so that the block count is set by registers */
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  if (smem > 48 * 1024)
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaSuccess;
+}
+
+template <typename K>
+static cudaError_t occupancy_of(K kernel, int block, size_t smem, int* bps) {
+  cudaError_t e = occupancy_smem_attr(kernel, smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, kernel, block, smem);
+}
+
+cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t smem, int* blocks_per_sm) {
+  if (algorithm == kAlgorithmEventsDense)
+    return counters ? occupancy_of(transport_events_kernel<true, 4>, block, smem, blocks_per_sm)
+                    : occupancy_of(transport_events_kernel<false, 4>, block, smem, blocks_per_sm);
+  if (algorithm == kAlgorithmEvents)
+    return counters ? occupancy_of(transport_events_kernel<true>, block, smem, blocks_per_sm)
+                    : occupancy_of(transport_events_kernel<false>, block, smem, blocks_per_sm);
+  return counters ? occupancy_of(transport_kernel<true>, block, smem, blocks_per_sm)
+                  : occupancy_of(transport_kernel<false>, block, smem, blocks_per_sm);
 }
 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                             bool counters, int grid, int block, size_t smem, cudaStream_t stream) {
-  if (smem > 48 * 1024) {
-    cudaError_t e = counters ? cudaFuncSetAttribute(transport_kernel<true>,
-                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                             : cudaFuncSetAttribute(transport_kernel<false>,
-                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+                             bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream) {
+  if (algorithm == kAlgorithmEventsDense) {
+    if (counters) transport_events_kernel<true, 4><<<grid, block, smem, stream>>>(P, T, O);
+    else transport_events_kernel<false, 4><<<grid, block, smem, stream>>>(P, T, O);
+  } else if (algorithm == kAlgorithmEvents) {
+    if (counters) transport_events_kernel<true><<<grid, block, smem, stream>>>(P, T, O);
+    else transport_events_kernel<false><<<grid, block, smem, stream>>>(P, T, O);
+  } else {
+    if (counters) transport_kernel<true><<<grid, block, smem, stream>>>(P, T, O);
+    else transport_kernel<false><<<grid, block, smem, stream>>>(P, T, O);
   }
-  if (counters) transport_kernel<true><<<grid, block, smem, stream>>>(P, T, O);
-  else transport_kernel<false><<<grid, block, smem, stream>>>(P, T, O);
   return cudaGetLastError();
 }
+
 
 cudaError_t launch_probe_rng(const TransportParams& P, int n, const int64_t* ids, int ndraw, int2* seeds,
                              float* draws, double* ddraws, cudaStream_t s) {

@@ -8,11 +8,15 @@
 
 namespace mcpet {
 
-size_t transport_dynamic_smem(const TransportParams& P, int block);
+constexpr int kAlgorithmHistories = 1;  /* one lane per thread, history after history */
+constexpr int kAlgorithmEvents = 2;     /* warp-regrouped event loop */
+constexpr int kAlgorithmEventsDense = 3;/* same, compiled for 4 resident blocks per SM */
+
+size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();
-cudaError_t transport_occupancy(bool counters, int block, size_t smem, int* blocks_per_sm);
+cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t smem, int* blocks_per_sm);
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                             bool counters, int grid, int block, size_t smem, cudaStream_t stream);
+                             bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream);
 
 cudaError_t launch_probe_rng(const TransportParams& P, int n, const int64_t* ids, int ndraw, int2* seeds,
                              float* draws, double* ddraws, cudaStream_t s);

@@ -90,6 +90,9 @@ struct TransportParams {
   int palette_in_shared;  /* palette size if staged in shared memory, else 0 */
   int spectrum_in_shared; /* 1 when ne <= kSpectrumSharedMax */
   int max_shells;         /* largest noscco over used materials */
+  float e_annihilation;   /* 510998.95 eV, passed at run time */
+  int quorum_scatter;     /* event loop: lanes needed to run a scattering round */
+  int quorum_pair;        /* ... and a pair-bookkeeping (end of photon, next decay) round */
 };
 
 /* Device pointers of one scene (all read-only during transport). */

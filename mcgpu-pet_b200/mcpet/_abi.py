@@ -18,6 +18,10 @@ PSF_RECORD_BYTES = 44
 LANES_REFERENCE = 0
 LANES_BALANCED = 1
 
+ALGORITHM_AUTO = 0
+ALGORITHM_HISTORIES = 1
+ALGORITHM_EVENTS = 2
+
 STATUS_NAMES = {
     0: "MCPET_OK",
     1: "MCPET_ERR_ARG",
@@ -110,6 +114,7 @@ class RunOpts(C.Structure):
         ("collect_counters", C.c_int),
         ("seed_override", C.c_int),
         ("stream", C.c_void_p),
+        ("algorithm", C.c_int),
     ]
 
 

@@ -36,6 +36,7 @@ class RunOptions:
     collect_counters: bool = False
     seed_override: int = 0
     stream: int = 0
+    algorithm: int = _abi.ALGORITHM_AUTO
 
     def to_c(self) -> _abi.RunOpts:
         o = _abi.RunOpts()
@@ -47,6 +48,7 @@ class RunOptions:
         o.collect_counters = int(bool(self.collect_counters))
         o.seed_override = int(self.seed_override)
         o.stream = self.stream or None
+        o.algorithm = int(self.algorithm)
         return o
 
 
