@@ -221,6 +221,31 @@ mcpet_status mcpet_run(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_tal
 mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
                               mcpet_tallies* device_out);
 
+/* Allocation-free variant of mcpet_run_device, for callers that may not
+ * allocate device memory while they run: plugin or custom-call hooks inside a
+ * host framework that hands out every device buffer from its own pool, and
+ * stream pipelines that cannot afford the device-wide synchronisation that
+ * cudaMalloc/cudaFree imply.  No counterpart in the reference (its program
+ * allocates everything in init_CUDA_device).
+ *
+ * The caller passes the per-voxel activity (float, n_voxels, device memory)
+ * and the device output buffers of mcpet_tallies.  The scene's tables must
+ * already be on the device (mcpet_scene_to_device, done once at set-up, is
+ * the call that allocates).  The lane plan and the work-queue words are
+ * built in a fixed static device array of the library instead of allocated
+ * buffers: it holds plans of up to MCPET_NOALLOC_MAX_VOXELS voxels (about
+ * 32 MiB) and every GPU that loads the library reserves it until the process
+ * exits.  Larger phantoms are rejected with MCPET_ERR_LIMIT.  All calls on a
+ * device share that array and rewrite it, so calls that overlap on the GPU
+ * (several streams or threads at once) race; serialise them.  The first call
+ * on a device looks up the array's device address; make that first call
+ * before any stream capture.  Lanes are laid out in voxel order: with
+ * MCPET_LANES_REFERENCE the results equal mcpet_run_device's.  Guard trips
+ * are reported only through device_out->counters (collect_counters=1). */
+#define MCPET_NOALLOC_MAX_VOXELS (1 << 20)
+mcpet_status mcpet_run_device_noalloc(mcpet_scene* scene, const float* activity_device,
+                                      const mcpet_run_opts* opts, mcpet_tallies* device_out);
+
 /* Device-side guard status of the last run on this scene (blocking read). */
 mcpet_status mcpet_last_run_guard(mcpet_scene* scene, unsigned long long* trips);
 

@@ -675,6 +675,75 @@ mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallie
   return MCPET_OK;
 }
 
+mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_device, const mcpet_run_opts* opts,
+                                      mcpet_tallies* out) {
+  if (!sc || !activity_device || !out) return set_error(MCPET_ERR_ARG, "null argument");
+  const long long nv = (long long)sc->mat0.size();
+  if (nv > MCPET_NOALLOC_MAX_VOXELS || nv > kNoAllocMaxVoxels)
+    return set_error(MCPET_ERR_LIMIT,
+                     "phantom has %lld voxels; the allocation-free run holds lane plans of at most %d voxels "
+                     "(use mcpet_run_device)", nv, (int)kNoAllocMaxVoxels);
+  mcpet_status s = validate_opts(sc, opts);
+  if (s != MCPET_OK) return s;
+  auto& d = sc->dev;
+  if (d.device < 0 || !d.tables_ready)
+    return set_error(MCPET_ERR_ARG, "the scene is not on a device: call mcpet_scene_to_device first (it allocates)");
+  CUDA_TRY(cudaSetDevice(d.device));
+  mcpet_run_opts def;
+  memset(&def, 0, sizeof(def));
+  const mcpet_run_opts& o = opts ? *opts : def;
+  const bool sino = sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 2;
+  if (sino && (!out->trues || !out->scatter || !out->image_trues || !out->image_scatter || !out->spectrum))
+    return set_error(MCPET_ERR_ARG, "sinogram tally requested but a sinogram/image/spectrum buffer is missing");
+  if (!out->total_histories || !out->psf_count) return set_error(MCPET_ERR_ARG, "histories and psf_count are required");
+
+  TransportParams P;
+  fill_params(sc, P);
+  if (o.seed_override != 0) P.seed = o.seed_override;
+  P.background_mode = o.background_mode ? 1 : 0;
+  if (!out->psf) P.psf_capacity = 0;
+  else P.psf_capacity = (int)std::min<long long>(out->psf_capacity, 0x7fffffff);
+  if (!sino) P.spectrum_in_shared = 0;
+  const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
+  int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
+
+  DeviceTallies O;
+  memset(&O, 0, sizeof(O));
+  O.trues = out->trues;
+  O.scatter = out->scatter;
+  O.image_trues = out->image_trues;
+  O.image_scatter = out->image_scatter;
+  O.spectrum = out->spectrum;
+  O.psf = (uint32_t*)out->psf;
+  O.psf_count = out->psf_count;
+  O.histories = out->total_histories;
+  O.coincidences = out->coincidences;
+  O.counters = (unsigned long long*)out->counters;
+  cudaStream_t st = (cudaStream_t)o.stream;
+  const size_t nb = (size_t)sc->cfg.n_bins * 4, nvb = (size_t)nv * 4;
+  if (O.trues) CUDA_TRY(cudaMemsetAsync(O.trues, 0, nb, st));
+  if (O.scatter) CUDA_TRY(cudaMemsetAsync(O.scatter, 0, nb, st));
+  if (O.image_trues) CUDA_TRY(cudaMemsetAsync(O.image_trues, 0, nvb, st));
+  if (O.image_scatter) CUDA_TRY(cudaMemsetAsync(O.image_scatter, 0, nvb, st));
+  if (O.spectrum) CUDA_TRY(cudaMemsetAsync(O.spectrum, 0, (size_t)sc->cfg.n_energy_bins * 4, st));
+  CUDA_TRY(cudaMemsetAsync(O.psf_count, 0, 4, st));
+  CUDA_TRY(cudaMemsetAsync(O.histories, 0, 8, st));
+  if (O.coincidences) CUDA_TRY(cudaMemsetAsync(O.coincidences, 0, 8, st));
+  const bool counters = o.collect_counters && O.counters;
+  if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
+
+  int block = transport_block_threads();
+  size_t smem = transport_dynamic_smem(P, block, kAlgorithmEvents);
+  int bps = 0;
+  CUDA_TRY(transport_occupancy(counters, kAlgorithmEvents, block, smem, &bps));
+  if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
+  if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
+  const int grid = d.sm_count * bps;
+  CUDA_TRY(launch_transport_noalloc(P, device_tables(sc), O, activity_device, o.lane_mode, tpb, hpl, counters,
+                                    grid, block, smem, st));
+  return MCPET_OK;
+}
+
 mcpet_status mcpet_last_run_guard(mcpet_scene* sc, unsigned long long* trips) {
   if (!sc || !trips) return set_error(MCPET_ERR_ARG, "null argument");
   if (sc->dev.device < 0 || !sc->dev.small) {

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 
 #include "mcpet_device.cuh"
 #include "mcpet_kernels.h"
@@ -424,11 +425,13 @@ struct ColdState {
 };
 
 
-template <bool kCount, int kMinBlocks = 1>
+template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(TransportParams P, DeviceTables T,
                                                                               DeviceTallies O) {
-  const uint64_t n_lanes = P.n_lanes;
-  const int n_emitters = P.n_emitters;
+  /* kDevicePlan: the lane plan was built on the device and its size is read
+   * from device memory instead of the launch parameters */
+  const uint64_t n_lanes = kDevicePlan ? (uint64_t)O.plan_counts[0] : P.n_lanes;
+  const int n_emitters = kDevicePlan ? (int)O.plan_counts[1] : P.n_emitters;
   __shared__ ComptonTable cmp;
   __shared__ float s0_ann[kMaxMaterials];
   extern __shared__ float4 dyn_smem[];
@@ -835,6 +838,175 @@ __global__ void probe_source_kernel(TransportParams P, int background, int2* see
   seeds[v] = make_int2(r.x, r.y);
 }
 
+/* ------------------------------------------------ allocation-free runs
+ *
+ * Scratch of mcpet_run_device_noalloc: the lane plan (built on the device
+ * from the caller's activity map) and the work-queue words live in this one
+ * file-scope device array instead of library allocations.  Its size is fixed
+ * at build time (kNoAllocMaxVoxels emitters of 32 bytes plus a small header,
+ * about 32 MiB) and every GPU that loads the library holds it until the
+ * process exits.  All calls on a device share it: calls that overlap on the
+ * GPU race on it.  Each call rewrites the header and the plan it uses. */
+
+constexpr int kPlanChunk = 4096;                                  /* voxels per plan block */
+constexpr int kPlanMaxChunks = kNoAllocMaxVoxels / kPlanChunk;
+
+struct NoAllocScratch {
+  unsigned long long header[8];   /* 0 lane cursor, 1 guard, 2 lanes, 3 emitters, 4 coincidences (fallback) */
+  unsigned long long chunk_lanes[kPlanMaxChunks];
+  unsigned int chunk_emitters[kPlanMaxChunks];
+  Emitter plan[kNoAllocMaxVoxels];
+};
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+namespace {
+
+__device__ __forceinline__ unsigned long long plan_lanes_of(float a, int mode, int tpb, double t_s, int hpl) {
+  if (mode == 0) return (unsigned long long)tpb;
+  double L = ceil((double)a * t_s / (double)hpl);
+  if (L < 1) L = 1;
+  if (L > 1.0e8) L = 1.0e8;
+  return (unsigned long long)L;
+}
+
+/* per chunk of voxels: number of emitters and of lanes */
+__global__ void plan_count_kernel(const float* act, int nvox, int mode, int tpb, double t_s, int hpl,
+                                  NoAllocScratch* S) {
+  __shared__ unsigned long long sl[32];
+  __shared__ unsigned int se[32];
+  const int v0 = blockIdx.x * kPlanChunk, v1 = min(v0 + kPlanChunk, nvox);
+  unsigned int ne = 0;
+  unsigned long long nl = 0;
+  for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+    float a = act[v];
+    if (a > 1.0e-7f) {
+      ne += 1;
+      nl += plan_lanes_of(a, mode, tpb, t_s, hpl);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ne += __shfl_down_sync(0xffffffffu, ne, o);
+    nl += __shfl_down_sync(0xffffffffu, nl, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    se[threadIdx.x >> 5] = ne;
+    sl[threadIdx.x >> 5] = nl;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int te = 0;
+    unsigned long long tl = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      te += se[w];
+      tl += sl[w];
+    }
+    S->chunk_emitters[blockIdx.x] = te;
+    S->chunk_lanes[blockIdx.x] = tl;
+  }
+}
+
+/* exclusive prefix over the chunks, totals, and the words that start at zero */
+__global__ void plan_scan_kernel(int n_chunks, NoAllocScratch* S) {
+  if (threadIdx.x != 0) return;
+  unsigned long long lanes = 0;
+  unsigned int emitters = 0;
+  for (int c = 0; c < n_chunks; ++c) {
+    unsigned long long l = S->chunk_lanes[c];
+    unsigned int e = S->chunk_emitters[c];
+    S->chunk_lanes[c] = lanes;
+    S->chunk_emitters[c] = emitters;
+    lanes += l;
+    emitters += e;
+  }
+  S->header[0] = 0;      /* lane cursor */
+  S->header[1] = 0;      /* guard trips */
+  S->header[4] = 0;      /* coincidence fallback counter */
+  if (lanes >= (1ull << 31)) {
+    /* more RANECU streams than the reference's 31-bit thread ids: run nothing
+     * and count a guard trip */
+    S->header[1] = 1;
+    lanes = 0;
+    emitters = 0;
+  }
+  S->header[2] = lanes;
+  S->header[3] = emitters;
+}
+
+/* emitter records in voxel order (one block per chunk, block-wide scans) */
+__global__ void plan_fill_kernel(const float* act, int nvox, int mode, int tpb, double t_s, int hpl,
+                                 NoAllocScratch* S) {
+  __shared__ unsigned int we[32];
+  __shared__ unsigned long long wl[32];
+  __shared__ unsigned int run_e;
+  __shared__ unsigned long long run_l;
+  const int c = blockIdx.x;
+  const int v0 = c * kPlanChunk, v1 = min(v0 + kPlanChunk, nvox);
+  if (threadIdx.x == 0) {
+    run_e = S->chunk_emitters[c];
+    run_l = S->chunk_lanes[c];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = v0; base < v1; base += blockDim.x) {
+    const int v = base + threadIdx.x;
+    float a = (v < v1) ? act[v] : 0.0f;
+    const bool emit = a > 1.0e-7f;
+    unsigned int e = emit ? 1u : 0u;
+    unsigned long long l = emit ? plan_lanes_of(a, mode, tpb, t_s, hpl) : 0ull;
+    /* inclusive warp scans */
+    unsigned int ie = e;
+    unsigned long long il = l;
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned int te = __shfl_up_sync(0xffffffffu, ie, o);
+      unsigned long long tl = __shfl_up_sync(0xffffffffu, il, o);
+      if (lane >= o) {
+        ie += te;
+        il += tl;
+      }
+    }
+    if (lane == 31) {
+      we[warp] = ie;
+      wl[warp] = il;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned int acc_e = 0;
+      unsigned long long acc_l = 0;
+      for (int w = 0; w < nw; ++w) {
+        unsigned int te = we[w];
+        unsigned long long tl = wl[w];
+        we[w] = acc_e;
+        wl[w] = acc_l;
+        acc_e += te;
+        acc_l += tl;
+      }
+      we[31] = acc_e;           /* tile totals (nw <= 8 < 31) */
+      wl[31] = acc_l;
+    }
+    __syncthreads();
+    if (emit) {
+      const unsigned int rank = run_e + we[warp] + (ie - e);
+      const unsigned long long first = run_l + wl[warp] + (il - l);
+      Emitter em;
+      em.inv_rate = (double)l / (double)a;
+      em.voxel = (uint32_t)v;
+      em.n_lanes = (uint32_t)l;
+      em.first_lane = first;
+      em.stream_base = (mode == 0) ? (uint64_t)v * (uint64_t)tpb : first;
+      S->plan[rank] = em;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      run_e += we[31];
+      run_l += wl[31];
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 /* ---------------------------------------------------------- launchers */
@@ -894,6 +1066,57 @@ cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, co
   return cudaGetLastError();
 }
 
+/* Device address of the scratch array, looked up once per device with that
+ * device current (the array's host-side name is only a stand-in). */
+static std::mutex g_scratch_mutex;
+static void* g_scratch_ptr[128];
+
+static cudaError_t noalloc_scratch(NoAllocScratch** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_ptr[dev] = p;
+  }
+  *out = static_cast<NoAllocScratch*>(g_scratch_ptr[dev]);
+  return cudaSuccess;
+}
+
+cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,
+                                     const float* activity, int lane_mode, int tpb, int hpl, bool counters,
+                                     int grid, int block, size_t smem, cudaStream_t stream) {
+  NoAllocScratch* S = nullptr;
+  cudaError_t e = noalloc_scratch(&S);
+  if (e != cudaSuccess) return e;
+  const int nvox = (int)P.n_voxels;
+  if (nvox <= 0 || nvox > kNoAllocMaxVoxels) return cudaErrorInvalidValue;
+  const int n_chunks = (nvox + kPlanChunk - 1) / kPlanChunk;
+  const double t_s = (double)P.acq_ps * 1e-12;
+  plan_count_kernel<<<n_chunks, 256, 0, stream>>>(activity, nvox, lane_mode, tpb, t_s, hpl, S);
+  plan_scan_kernel<<<1, 32, 0, stream>>>(n_chunks, S);
+  plan_fill_kernel<<<n_chunks, 256, 0, stream>>>(activity, nvox, lane_mode, tpb, t_s, hpl, S);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  T.emitters = S->plan;
+  O.lane_cursor = &S->header[0];
+  O.guard = &S->header[1];
+  O.plan_counts = &S->header[2];
+  if (!O.coincidences) O.coincidences = &S->header[4];
+  if (counters) {
+    e = occupancy_smem_attr(transport_events_kernel<true, 1, true>, smem);
+    if (e == cudaSuccess) transport_events_kernel<true, 1, true><<<grid, block, smem, stream>>>(P, T, O);
+  } else {
+    e = occupancy_smem_attr(transport_events_kernel<false, 1, true>, smem);
+    if (e == cudaSuccess) transport_events_kernel<false, 1, true><<<grid, block, smem, stream>>>(P, T, O);
+  }
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_probe_rng(const TransportParams& P, int n, const int64_t* ids, int ndraw, int2* seeds,
                              float* draws, double* ddraws, cudaStream_t s) {

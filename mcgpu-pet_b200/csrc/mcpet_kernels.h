@@ -18,6 +18,12 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream);
 
+/* allocation-free runs: lane plan and work-queue words in a static device array */
+constexpr int kNoAllocMaxVoxels = 1 << 20;
+cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,
+                                     const float* activity, int lane_mode, int tpb, int hpl, bool counters,
+                                     int grid, int block, size_t smem, cudaStream_t stream);
+
 cudaError_t launch_probe_rng(const TransportParams& P, int n, const int64_t* ids, int ndraw, int2* seeds,
                              float* draws, double* ddraws, cudaStream_t s);
 cudaError_t launch_probe_detector(const TransportParams& P, int n, const float* e2, const float* e1,

@@ -122,6 +122,7 @@ struct DeviceTallies {
   unsigned long long* counters;   /* 10 counters (mcpet_counters order) or NULL */
   unsigned long long* guard;      /* guard trips */
   unsigned long long* lane_cursor;/* lane work queue head */
+  const unsigned long long* plan_counts; /* [lanes, emitters] on the device (device-built plans) */
 };
 
 }  // namespace mcpet
