@@ -331,7 +331,8 @@ def main():
     achieved = b_alg / (avg_kernel_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "peak_kind": peak_kind,
-            "kernel": "transport_kernel", "kernel_ms": avg_kernel_ms, "algorithmic_bytes_per_launch": b_alg,
+            "kernel": "transport_kernel" if args.algorithm == "histories" else "transport_events_kernel",
+            "kernel_ms": avg_kernel_ms, "algorithmic_bytes_per_launch": b_alg,
             "counters": counters}
     prof = os.path.join(ROOT, "profiles", "transport_traffic.json")
     if os.path.exists(prof):
@@ -349,7 +350,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded head phantom, random-free tables from the reference's air/water data)",
+                "data": "synthetic (seeded head phantom; tissue densities on the reference's own air/water material tables)",
                 "config": {"workload": WORKLOAD, "emissions_per_step_per_gpu": args.emissions,
                            "lanes": args.lanes, "algorithm": args.algorithm, "parallelism": f"replicas x{world}",
                            "l2": "each step zeroes 4.2 GB of sinograms (> 126 MB L2) before the kernel",

@@ -131,8 +131,8 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.spectrum_in_shared = (c.n_energy_bins > 0 && c.n_energy_bins <= kSpectrumSharedMax) ? 1 : 0;
   P.palette_in_shared = (sc->palette.size() <= 2048) ? (int)sc->palette.size() : 0;
   P.e_annihilation = 510998.95f;
-  P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 24, 1, 32);
-  P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 8, 1, 32);
+  P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 16, 1, 32);
+  P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 32, 1, 32);
 }
 
 mcpet_status upload_tables(mcpet_scene* sc) {
@@ -367,7 +367,7 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   block = (block / 32) * 32;
   if (block < 32) block = 32;
   int algorithm = o.algorithm == kAlgorithmHistories ? kAlgorithmHistories : kAlgorithmEvents;
-  if (algorithm == kAlgorithmEvents && env_int("MCPET_DENSE", 0, 0, 1)) algorithm = kAlgorithmEventsDense;
+  if (algorithm == kAlgorithmEvents && env_int("MCPET_MINBLOCKS", 4, 1, 4) == 1) algorithm = kAlgorithmEventsUncapped;
   size_t smem = transport_dynamic_smem(P, block, algorithm);
   int bps = 0;
   CUDA_TRY(transport_occupancy(counters, algorithm, block, smem, &bps));

@@ -1040,11 +1040,16 @@ static cudaError_t occupancy_of(K kernel, int block, size_t smem, int* bps) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, kernel, block, smem);
 }
 
+/* The event kernel is compiled with its registers capped so that kEventBlocks
+ * blocks of 256 threads stay resident per SM (a few spilled words cost less
+ * than the lost warps); kAlgorithmEventsUncapped keeps the uncapped build. */
+constexpr int kEventBlocks = 4;
+
 cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t smem, int* blocks_per_sm) {
-  if (algorithm == kAlgorithmEventsDense)
-    return counters ? occupancy_of(transport_events_kernel<true, 4>, block, smem, blocks_per_sm)
-                    : occupancy_of(transport_events_kernel<false, 4>, block, smem, blocks_per_sm);
   if (algorithm == kAlgorithmEvents)
+    return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks>, block, smem, blocks_per_sm)
+                    : occupancy_of(transport_events_kernel<false, kEventBlocks>, block, smem, blocks_per_sm);
+  if (algorithm == kAlgorithmEventsUncapped)
     return counters ? occupancy_of(transport_events_kernel<true>, block, smem, blocks_per_sm)
                     : occupancy_of(transport_events_kernel<false>, block, smem, blocks_per_sm);
   return counters ? occupancy_of(transport_kernel<true>, block, smem, blocks_per_sm)
@@ -1053,10 +1058,10 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t 
 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream) {
-  if (algorithm == kAlgorithmEventsDense) {
-    if (counters) transport_events_kernel<true, 4><<<grid, block, smem, stream>>>(P, T, O);
-    else transport_events_kernel<false, 4><<<grid, block, smem, stream>>>(P, T, O);
-  } else if (algorithm == kAlgorithmEvents) {
+  if (algorithm == kAlgorithmEvents) {
+    if (counters) transport_events_kernel<true, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O);
+    else transport_events_kernel<false, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O);
+  } else if (algorithm == kAlgorithmEventsUncapped) {
     if (counters) transport_events_kernel<true><<<grid, block, smem, stream>>>(P, T, O);
     else transport_events_kernel<false><<<grid, block, smem, stream>>>(P, T, O);
   } else {
@@ -1108,11 +1113,11 @@ cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, D
   O.plan_counts = &S->header[2];
   if (!O.coincidences) O.coincidences = &S->header[4];
   if (counters) {
-    e = occupancy_smem_attr(transport_events_kernel<true, 1, true>, smem);
-    if (e == cudaSuccess) transport_events_kernel<true, 1, true><<<grid, block, smem, stream>>>(P, T, O);
+    e = occupancy_smem_attr(transport_events_kernel<true, kEventBlocks, true>, smem);
+    if (e == cudaSuccess) transport_events_kernel<true, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O);
   } else {
-    e = occupancy_smem_attr(transport_events_kernel<false, 1, true>, smem);
-    if (e == cudaSuccess) transport_events_kernel<false, 1, true><<<grid, block, smem, stream>>>(P, T, O);
+    e = occupancy_smem_attr(transport_events_kernel<false, kEventBlocks, true>, smem);
+    if (e == cudaSuccess) transport_events_kernel<false, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O);
   }
   if (e != cudaSuccess) return e;
   return cudaGetLastError();

@@ -9,8 +9,8 @@
 namespace mcpet {
 
 constexpr int kAlgorithmHistories = 1;  /* one lane per thread, history after history */
-constexpr int kAlgorithmEvents = 2;     /* warp-regrouped event loop */
-constexpr int kAlgorithmEventsDense = 3;/* same, compiled for 4 resident blocks per SM */
+constexpr int kAlgorithmEvents = 2;     /* warp-regrouped event loop, registers capped for occupancy */
+constexpr int kAlgorithmEventsUncapped = 3; /* same loop, registers not capped (MCPET_MINBLOCKS=1) */
 
 size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();
