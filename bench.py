@@ -193,6 +193,47 @@ def run_reference_arm(args):
     return 0
 
 
+def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8) -> dict:
+    """Batched many-phantom workload: one mcpet_run_batch launch against the
+    same scenes run one after another (mcpet_run), same options and seeds.
+    Both give identical tallies; times are the transport kernels' (CUDA
+    events) and the wall clock of the host calls."""
+    import mcpet
+    from mcpet import inputs
+    sc, sizes = [], []
+    for k, (mat, rho, act, vs, used) in enumerate(inputs.batch_phantoms(n_scenes, emissions_each)):
+        spec = inputs.spec_for(inputs.tissue_materials(list(inputs.TISSUES)[:8]), "unused.vox", seed=1000 + k,
+                               **inputs.scanner_batch())
+        cfg = inputs.config_from_spec(spec, workdir)
+        sc.append(mcpet.Scene.from_arrays(cfg, mat, rho, act, vs))
+        sizes.append(mat.shape[0])
+    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED)
+    for s in sc:                                  # warm-up: device tables, run buffers
+        s.run(opts)
+    mcpet.Scene.run_batch(sc, opts)
+    t0 = time.perf_counter()
+    seq = [s.run(opts) for s in sc]
+    seq_wall = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bat = mcpet.Scene.run_batch(sc, opts)
+    bat_wall = time.perf_counter() - t0
+    coinc = sum(r.detected for r in bat)
+    identical = all(a.detected == b.detected and a.total_histories == b.total_histories and
+                    bool((a.trues == b.trues).all()) for a, b in zip(seq, bat))
+    seq_ms = sum(r.transport_ms for r in seq)
+    bat_ms = bat[0].transport_ms
+    for s in sc:
+        s.close()
+    return {"workload": f"{n_scenes} head-like phantoms of m^3 voxels, m in [32,192] (min {min(sizes)}, max "
+                        f"{max(sizes)}), 2-4 mm voxels, {emissions_each:.0e} decays each; scanner 32 rings, "
+                        "128 rad x 128 ang x 1985 planes (span 1)",
+            "coincidences": coinc, "identical_to_sequential": identical,
+            "batched_kernel_ms": bat_ms, "sequential_kernel_ms": seq_ms,
+            "batched_value": coinc / (bat_ms * 1e-3), "sequential_value": coinc / (seq_ms * 1e-3),
+            "batched_wall_s": bat_wall, "sequential_wall_s": seq_wall,
+            "kernel_speedup": seq_ms / bat_ms, "wall_speedup": seq_wall / bat_wall, "unit": UNIT}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,6 +246,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--algorithm", default="auto", choices=["auto", "histories", "events"])
+    ap.add_argument("--batch-scenes", type=int, default=0,
+                    help="also time N phantoms of m^3 voxels (m in [32,192], 1e8 decays each) batched in one "
+                         "launch against the same runs one by one (reported under 'batch')")
+    ap.add_argument("--batch-emissions", type=float, default=1.0e8, help="decays per phantom of --batch-scenes")
     ap.add_argument("--scanner", default="head", choices=["head", "head32"],
                     help="head32: smaller sinogram for profiler captures (not a bench line)")
     args = ap.parse_args()
@@ -341,6 +386,10 @@ def main():
         except Exception:
             pass
 
+    batch = None
+    if args.batch_scenes > 0 and rank == 0:
+        batch = measure_batch(args.batch_scenes, tmp, args.batch_emissions)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, desc, _, _ = cpu_reference_sample(cfg, mat, rho, act, vs, args.cpu_seconds)
@@ -357,6 +406,8 @@ def main():
                            "coincidences_per_step": total / args.steps / world, "histories_last_step": hist,
                            "guard_trips": guard},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks}
+        if batch is not None:
+            line["batch"] = batch
         print(json.dumps(line))
     scene.close()
     if dist:

@@ -221,6 +221,29 @@ mcpet_status mcpet_run(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_tal
 mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
                               mcpet_tallies* device_out);
 
+/* Batched run: the lanes of n_scenes scenes (phantoms of any size, each with
+ * its own activity, seed, acquisition time and isotope mean life) in ONE
+ * persistent launch of the transport kernel, so the GPU stays full through
+ * the tail of every scene.  Replaces n_scenes sequential runs of the
+ * reference program (MCGPU-PET.cu:77-840, one phantom per process).  Each
+ * scene keeps its own lane plan and RANECU streams: its tallies equal those
+ * of mcpet_run on that scene alone with the same options.  The scenes must
+ * use the same material files in the same slots (the Compton and Rayleigh
+ * tables are shared by the launch) and sit on one device (scenes not yet on
+ * a device are placed on scene 0's).  opts applies to every scene
+ * (algorithm 0 or 2 only).  outs[k] receives scene k's tallies as in
+ * mcpet_run; counters, when requested, are totals of the launch and go to
+ * outs[0], and mcpet_last_run_guard(scenes[0]) reports the launch's guard
+ * trips.  Blocking. */
+mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                             mcpet_tallies* outs);
+
+/* Batched run into DEVICE tallies (device_outs[k] as in mcpet_run_device),
+ * ordered on opts->stream; the merged lane plan is uploaded and released in
+ * stream order. */
+mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                                    mcpet_tallies* device_outs);
+
 /* Allocation-free variant of mcpet_run_device, for callers that may not
  * allocate device memory while they run: plugin or custom-call hooks inside a
  * host framework that hands out every device buffer from its own pool, and

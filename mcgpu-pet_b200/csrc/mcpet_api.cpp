@@ -133,6 +133,7 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.e_annihilation = 510998.95f;
   P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 16, 1, 32);
   P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 32, 1, 32);
+  P.step_keep = env_int("MCPET_STEP_KEEP", 2, 1, 8);
 }
 
 mcpet_status upload_tables(mcpet_scene* sc) {
@@ -222,15 +223,11 @@ DeviceTables device_tables(const mcpet_scene* sc) {
 /* Lane plan: emitters (voxels with activity > 1e-7 Bq, the reference's
  * threshold at MCGPU-PET_kernel.cu:232) with their lane counts and RANECU
  * streams, ordered by decreasing expected decays per lane. */
-mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
-  auto& d = sc->dev;
-  char key[128];
-  snprintf(key, sizeof(key), "%d/%d/%d", mode, tpb, hpl);
-  if (!d.activity_dirty && d.plan_key == key && d.emitters) return MCPET_OK;
-  /* a new plan is built on the host from the activity map and uploaded */
+mcpet_status plan_host(const mcpet_scene* sc, int mode, int tpb, int hpl, std::vector<Emitter>& em,
+                       uint64_t& n_lanes) {
   const size_t nv = sc->activity.size();
   const double T = (double)sc->cfg.acquisition_time_ps * 1e-12;
-  std::vector<Emitter> em;
+  em.clear();
   em.reserve(1024);
   for (size_t v = 0; v < nv; ++v) {
     float a = sc->activity[v];
@@ -265,6 +262,20 @@ mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
   if (max_stream >= (1ull << 31))
     return set_error(MCPET_ERR_LIMIT, "lane plan needs %llu RANECU streams (limit 2^31)",
                      (unsigned long long)max_stream);
+  n_lanes = lanes;
+  return MCPET_OK;
+}
+
+mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
+  auto& d = sc->dev;
+  char key[128];
+  snprintf(key, sizeof(key), "%d/%d/%d", mode, tpb, hpl);
+  if (!d.activity_dirty && d.plan_key == key && d.emitters) return MCPET_OK;
+  /* a new plan is built on the host from the activity map and uploaded */
+  std::vector<Emitter> em;
+  uint64_t lanes = 0;
+  mcpet_status s = plan_host(sc, mode, tpb, hpl, em, lanes);
+  if (s != MCPET_OK) return s;
   if (em.size() > d.emitters_cap) {
     dfree(d.emitters);
     size_t cap = std::max<size_t>(em.size(), 1);
@@ -307,6 +318,43 @@ mcpet_status validate_opts(const mcpet_scene* sc, const mcpet_run_opts* opts) {
   return MCPET_OK;
 }
 
+/* Parameters of one scene's run and its zeroed outputs: everything but the
+ * lane plan and the launch.  O.coincidences defaults to a scene word. */
+mcpet_status prepare_run(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies& O, cudaStream_t st,
+                         TransportParams& P) {
+  fill_params(sc, P);
+  if (o.seed_override != 0) P.seed = o.seed_override;
+  if (P.seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", P.seed);
+  P.background_mode = o.background_mode ? 1 : 0;
+  if (!O.psf) P.psf_capacity = 0;
+
+  const bool sino = sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 2;
+  if (sino && (!O.trues || !O.scatter || !O.image_trues || !O.image_scatter || !O.spectrum))
+    return set_error(MCPET_ERR_ARG, "sinogram tally requested but a sinogram/image/spectrum buffer is missing");
+  if (!O.histories || !O.psf_count) return set_error(MCPET_ERR_ARG, "histories and psf_count are required");
+
+  const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
+  if (O.trues) CUDA_TRY(cudaMemsetAsync(O.trues, 0, nb, st));
+  if (O.scatter) CUDA_TRY(cudaMemsetAsync(O.scatter, 0, nb, st));
+  if (O.image_trues) CUDA_TRY(cudaMemsetAsync(O.image_trues, 0, nv, st));
+  if (O.image_scatter) CUDA_TRY(cudaMemsetAsync(O.image_scatter, 0, nv, st));
+  if (O.spectrum) CUDA_TRY(cudaMemsetAsync(O.spectrum, 0, (size_t)sc->cfg.n_energy_bins * 4, st));
+  CUDA_TRY(cudaMemsetAsync(O.psf_count, 0, 4, st));
+  CUDA_TRY(cudaMemsetAsync(O.histories, 0, 8, st));
+  if (!O.coincidences) O.coincidences = sc->dev.small + 14;
+  CUDA_TRY(cudaMemsetAsync(O.coincidences, 0, 8, st));
+  /* the kernel only touches the spectrum when the sinogram is tallied */
+  if (!sino) P.spectrum_in_shared = 0;
+  return MCPET_OK;
+}
+
+int pick_block(const mcpet_run_opts& o) {
+  int block = o.block_threads > 0 ? o.block_threads : transport_block_threads();
+  if (block > transport_block_threads()) block = transport_block_threads();
+  block = (block / 32) * 32;
+  return block < 32 ? 32 : block;
+}
+
 /* Enqueue one transport run writing into the device tallies O. */
 mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTallies O, cudaStream_t st,
                          double* ms_out) {
@@ -326,46 +374,20 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   if (s != MCPET_OK) return s;
 
   TransportParams P;
-  fill_params(sc, P);
-  if (o.seed_override != 0) P.seed = o.seed_override;
-  if (P.seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", P.seed);
-  P.background_mode = o.background_mode ? 1 : 0;
+  s = prepare_run(sc, o, O, st, P);
+  if (s != MCPET_OK) return s;
   P.n_lanes = sc->dev.n_lanes;
   P.n_emitters = sc->dev.n_emitters;
-  if (!O.psf) P.psf_capacity = 0;
-
-  const bool sino = sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 2;
-  if (sino && (!O.trues || !O.scatter || !O.image_trues || !O.image_scatter || !O.spectrum))
-    return set_error(MCPET_ERR_ARG, "sinogram tally requested but a sinogram/image/spectrum buffer is missing");
-  if (!O.histories || !O.psf_count) return set_error(MCPET_ERR_ARG, "histories and psf_count are required");
-  if (!P.spectrum_in_shared && !O.spectrum && sino) return set_error(MCPET_ERR_ARG, "spectrum buffer required");
 
   auto& d = sc->dev;
   unsigned long long* small = d.small;
   O.guard = small + 0;
   O.lane_cursor = small + 1;
   CUDA_TRY(cudaMemsetAsync(small, 0, 2 * sizeof(unsigned long long), st));
-  const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
-  if (O.trues) CUDA_TRY(cudaMemsetAsync(O.trues, 0, nb, st));
-  if (O.scatter) CUDA_TRY(cudaMemsetAsync(O.scatter, 0, nb, st));
-  if (O.image_trues) CUDA_TRY(cudaMemsetAsync(O.image_trues, 0, nv, st));
-  if (O.image_scatter) CUDA_TRY(cudaMemsetAsync(O.image_scatter, 0, nv, st));
-  if (O.spectrum) CUDA_TRY(cudaMemsetAsync(O.spectrum, 0, (size_t)sc->cfg.n_energy_bins * 4, st));
-  CUDA_TRY(cudaMemsetAsync(O.psf_count, 0, 4, st));
-  CUDA_TRY(cudaMemsetAsync(O.histories, 0, 8, st));
-  if (!O.coincidences) O.coincidences = small + 14;
-  CUDA_TRY(cudaMemsetAsync(O.coincidences, 0, 8, st));
   if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
-  if (!sino) {
-    /* the kernel only touches the spectrum when the sinogram is tallied */
-    P.spectrum_in_shared = 0;
-  }
 
   const bool counters = o.collect_counters && O.counters;
-  int block = o.block_threads > 0 ? o.block_threads : transport_block_threads();
-  if (block > transport_block_threads()) block = transport_block_threads();
-  block = (block / 32) * 32;
-  if (block < 32) block = 32;
+  const int block = pick_block(o);
   int algorithm = o.algorithm == kAlgorithmHistories ? kAlgorithmHistories : kAlgorithmEvents;
   if (algorithm == kAlgorithmEvents && env_int("MCPET_MINBLOCKS", 4, 1, 4) == 1) algorithm = kAlgorithmEventsUncapped;
   size_t smem = transport_dynamic_smem(P, block, algorithm);
@@ -443,6 +465,251 @@ mcpet_scene::~mcpet_scene() {
     if (dev.ev0) cudaEventDestroy((cudaEvent_t)dev.ev0);
     if (dev.ev1) cudaEventDestroy((cudaEvent_t)dev.ev1);
   }
+}
+
+/* Copy a finished host-buffer run (scene-owned device buffers) into out. */
+mcpet_status download_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out, bool want_psf, double ms,
+                          cudaStream_t st) {
+  auto& d = sc->dev;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
+  if (out->trues) CUDA_TRY(cudaMemcpyAsync(out->trues, d.trues, nb, cudaMemcpyDeviceToHost, st));
+  if (out->scatter) CUDA_TRY(cudaMemcpyAsync(out->scatter, d.scatter, nb, cudaMemcpyDeviceToHost, st));
+  if (out->image_trues) CUDA_TRY(cudaMemcpyAsync(out->image_trues, d.img_t, nv, cudaMemcpyDeviceToHost, st));
+  if (out->image_scatter) CUDA_TRY(cudaMemcpyAsync(out->image_scatter, d.img_s, nv, cudaMemcpyDeviceToHost, st));
+  if (out->spectrum)
+    CUDA_TRY(cudaMemcpyAsync(out->spectrum, d.spectrum, (size_t)sc->cfg.n_energy_bins * 4, cudaMemcpyDeviceToHost,
+                             st));
+  unsigned long long small[16];
+  CUDA_TRY(cudaMemcpyAsync(small, d.small, sizeof(small), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  int psf_count = (int)(small[3] & 0xffffffffull);
+  if (out->psf_count) *out->psf_count = psf_count;
+  if (out->total_histories) *out->total_histories = small[2];
+  if (out->coincidences) *out->coincidences = small[14];
+  if (want_psf) {
+    long long n = std::min<long long>(std::max(psf_count, 0), std::min<long long>(d.psf_cap, out->psf_capacity));
+    if (n > 0) CUDA_TRY(cudaMemcpy(out->psf, d.psf, (size_t)n * 44, cudaMemcpyDeviceToHost));
+  }
+  if (out->counters) {
+    memset(out->counters, 0, sizeof(mcpet_counters));
+    if (opts && opts->collect_counters) memcpy(out->counters, small + 4, 10 * 8);
+    out->counters->guard_trips = small[0];
+  }
+  if (out->transport_ms) *out->transport_ms = ms;
+  d.last_guard = small[0];
+  if (small[0] != 0)
+    return set_error(MCPET_ERR_DEVICE, "%llu device guard(s) fired (loop cap or out-of-range index)", small[0]);
+  return MCPET_OK;
+}
+
+
+/* Compton and Rayleigh data of a batched launch: the union of the material
+ * slots loaded by its scenes (a scene loads only the slots its phantom uses,
+ * as the reference does). */
+struct SharedTables {
+  ComptonTable cmp;
+  std::vector<float> ray;     /* xco|pco|aco|bco, [15*128] each */
+  std::vector<uint8_t> ray8;  /* itl|itu */
+};
+
+/* Builds the union; a slot loaded by two scenes must hold the same data. */
+mcpet_status merge_shared_tables(mcpet_scene* const* scenes, int n, SharedTables& U) {
+  const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
+  memset(&U.cmp, 0, sizeof(U.cmp));
+  U.ray.assign(4 * nr, 0.f);
+  U.ray8.assign(2 * nr, 0);
+  bool have[kMaxMaterials] = {false};
+  const mcpet_scene* a = scenes[0];
+  for (int k = 0; k < n; ++k) {
+    const mcpet_scene* b = scenes[k];
+    if (b->n_e != a->n_e || b->e0 != a->e0 || b->ide != a->ide)
+      return set_error(MCPET_ERR_ARG, "scene %d has another energy grid than scene 0 (first material file)", k);
+    for (int m = 0; m < kMaxMaterials; ++m) {
+      if (!b->material_loaded[m]) continue;
+      const int nsh = b->compton.noscco[m];
+      const float* rows[4] = {b->xco.data(), b->pco.data(), b->aco.data(), b->bco.data()};
+      const uint8_t* rows8[2] = {b->itl.data(), b->itu.data()};
+      if (have[m]) {
+        bool same = U.cmp.noscco[m] == nsh;
+        for (int i = 0; same && i < nsh; ++i) {
+          const int x = m + i * kMaxMaterials;
+          same = U.cmp.fco[x] == b->compton.fco[x] && U.cmp.uico[x] == b->compton.uico[x] &&
+                 U.cmp.fj0[x] == b->compton.fj0[x];
+        }
+        for (int r = 0; same && r < 4; ++r)
+          same = std::equal(rows[r] + m * kNpRayleigh, rows[r] + (m + 1) * kNpRayleigh,
+                            U.ray.begin() + r * nr + m * kNpRayleigh);
+        for (int r = 0; same && r < 2; ++r)
+          same = std::equal(rows8[r] + m * kNpRayleigh, rows8[r] + (m + 1) * kNpRayleigh,
+                            U.ray8.begin() + r * nr + m * kNpRayleigh);
+        if (!same)
+          return set_error(MCPET_ERR_ARG,
+                           "scene %d has other Compton/Rayleigh data in material slot %d than an earlier scene "
+                           "(the scenes of a batch must use the same material file in a slot)", k, m + 1);
+        continue;
+      }
+      have[m] = true;
+      U.cmp.noscco[m] = nsh;
+      for (int i = 0; i < nsh; ++i) {
+        const int x = m + i * kMaxMaterials;
+        U.cmp.fco[x] = b->compton.fco[x];
+        U.cmp.uico[x] = b->compton.uico[x];
+        U.cmp.fj0[x] = b->compton.fj0[x];
+      }
+      for (int r = 0; r < 4; ++r)
+        std::copy(rows[r] + m * kNpRayleigh, rows[r] + (m + 1) * kNpRayleigh, U.ray.begin() + r * nr + m * kNpRayleigh);
+      for (int r = 0; r < 2; ++r)
+        std::copy(rows8[r] + m * kNpRayleigh, rows8[r] + (m + 1) * kNpRayleigh,
+                  U.ray8.begin() + r * nr + m * kNpRayleigh);
+    }
+  }
+  return MCPET_OK;
+}
+
+/* Host-side checks of a batch (before any device work). */
+mcpet_status check_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts* opts, SharedTables* U) {
+  if (!scenes || n < 1) return set_error(MCPET_ERR_ARG, "a batch needs at least one scene");
+  if (n >= (1 << 23)) return set_error(MCPET_ERR_LIMIT, "batch of %d scenes (limit 2^23)", n);
+  if (opts && opts->algorithm == kAlgorithmHistories)
+    return set_error(MCPET_ERR_ARG, "batched runs use the event loop (algorithm 0 or 2)");
+  for (int k = 0; k < n; ++k) {
+    if (!scenes[k]) return set_error(MCPET_ERR_ARG, "scene %d of the batch is null", k);
+    mcpet_status s = validate_opts(scenes[k], opts);
+    if (s != MCPET_OK) return s;
+  }
+  SharedTables local;
+  return merge_shared_tables(scenes, n, U ? *U : local);
+}
+
+/* Enqueue ONE launch of the event kernel over the lanes of all scenes.
+ * outs[k] are scene k's device tallies.  Each scene keeps its own lane plan
+ * (cached on the scene like a single run's), seed and RANECU stream numbers,
+ * so its tallies equal those of a run of that scene alone. */
+mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts* opts, DeviceTallies* outs,
+                           cudaStream_t st, double* ms_out) {
+  SharedTables U;
+  mcpet_status cs = check_batch(scenes, n, opts, &U);
+  if (cs != MCPET_OK) return cs;
+  if (!outs) return set_error(MCPET_ERR_ARG, "null argument");
+  mcpet_run_opts def;
+  memset(&def, 0, sizeof(def));
+  const mcpet_run_opts& o = opts ? *opts : def;
+  mcpet_scene* s0 = scenes[0];
+  std::vector<SceneSlot> slots((size_t)n);
+  int max_shells = 1;
+  uint64_t total = 0;
+  for (int k = 0; k < n; ++k) {
+    mcpet_scene* sc = scenes[k];
+    sc->dev.run_h2d = 0;
+    mcpet_status s = MCPET_OK;
+    if (k > 0 && sc->dev.device < 0) s = mcpet_scene_to_device(sc, s0->dev.device);
+    else s = ensure_device(sc);
+    if (s != MCPET_OK) return s;
+    if (sc->dev.device != s0->dev.device)
+      return set_error(MCPET_ERR_ARG, "scene %d is on device %d, scene 0 on device %d", k, sc->dev.device,
+                       s0->dev.device);
+    s = upload_tables(sc);
+    if (s != MCPET_OK) return s;
+    const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
+    const int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
+    s = build_lanes(sc, o.lane_mode, tpb, hpl);
+    if (s != MCPET_OK) return s;
+    SceneSlot& z = slots[(size_t)k];
+    memset(&z, 0, sizeof(z));
+    z.O = outs[k];
+    s = prepare_run(sc, o, z.O, st, z.P);
+    if (s != MCPET_OK) return s;
+    z.P.spectrum_in_shared = 0;
+    z.P.palette_in_shared = 0;
+    z.P.n_lanes = sc->dev.n_lanes;
+    z.P.n_emitters = sc->dev.n_emitters;
+    z.T = device_tables(sc);
+    z.first_lane = total;
+    total += sc->dev.n_lanes;
+    max_shells = std::max(max_shells, z.P.max_shells);
+    CUDA_TRY(cudaMemsetAsync(sc->dev.small, 0, sizeof(unsigned long long), st));  /* guard word */
+  }
+  CUDA_TRY(cudaSetDevice(s0->dev.device));
+
+  /* per-call device data: the slots and the union tables, released in stream order */
+  const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
+  const size_t off_cmp = ((slots.size() * sizeof(SceneSlot) + 255) / 256) * 256;
+  const size_t off_ray = off_cmp + ((sizeof(ComptonTable) + 255) / 256) * 256;
+  const size_t off_ray8 = off_ray + 4 * nr * sizeof(float);
+  const size_t bytes = off_ray8 + 2 * nr;
+  std::vector<unsigned char> host(bytes, 0);
+  memcpy(host.data(), slots.data(), slots.size() * sizeof(SceneSlot));
+  memcpy(host.data() + off_cmp, &U.cmp, sizeof(ComptonTable));
+  memcpy(host.data() + off_ray, U.ray.data(), 4 * nr * sizeof(float));
+  memcpy(host.data() + off_ray8, U.ray8.data(), 2 * nr);
+  unsigned char* dbuf = nullptr;
+  CUDA_TRY(cudaMallocAsync((void**)&dbuf, bytes, st));
+  CUDA_TRY(cudaMemcpyAsync(dbuf, host.data(), bytes, cudaMemcpyHostToDevice, st));
+  for (int k = 0; k < n; ++k) scenes[k]->dev.last_h2d = scenes[k]->dev.run_h2d;
+  s0->dev.last_h2d += (long long)bytes;
+
+  /* launch-wide view: lane count, work queue and guard in scene 0's words */
+  TransportParams P = slots[0].P;
+  P.n_lanes = total;
+  P.n_emitters = 0;
+  P.max_shells = max_shells;
+  DeviceTables T = slots[0].T;
+  T.emitters = nullptr;
+  T.compton = reinterpret_cast<const ComptonTable*>(dbuf + off_cmp);
+  const float* ray = reinterpret_cast<const float*>(dbuf + off_ray);
+  T.rayleigh.xco = ray;
+  T.rayleigh.pco = ray + nr;
+  T.rayleigh.aco = ray + 2 * nr;
+  T.rayleigh.bco = ray + 3 * nr;
+  T.rayleigh.itl = dbuf + off_ray8;
+  T.rayleigh.itu = dbuf + off_ray8 + nr;
+  DeviceTallies O;
+  memset(&O, 0, sizeof(O));
+  O.guard = s0->dev.small + 0;
+  O.lane_cursor = s0->dev.small + 1;
+  CUDA_TRY(cudaMemsetAsync(O.lane_cursor, 0, sizeof(unsigned long long), st));
+  const bool counters = o.collect_counters && outs[0].counters;
+  if (counters) {
+    O.counters = outs[0].counters;
+    CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
+  }
+  const int block = pick_block(o);
+  const size_t smem = transport_dynamic_smem(P, block, kAlgorithmEvents);
+  int bps = 0;
+  CUDA_TRY(transport_batch_occupancy(counters, block, smem, &bps));
+  if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
+  if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
+  const int grid = total == 0 ? 1 : s0->dev.sm_count * bps;
+  auto& d = s0->dev;
+  if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
+  CUDA_TRY(launch_transport_batch(P, T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, counters, grid, block, smem,
+                                  st));
+  if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
+  CUDA_TRY(cudaFreeAsync(dbuf, st));
+  if (ms_out) {
+    CUDA_TRY(cudaEventSynchronize((cudaEvent_t)d.ev1));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, (cudaEvent_t)d.ev0, (cudaEvent_t)d.ev1));
+    *ms_out = ms;
+  }
+  return MCPET_OK;
+}
+
+DeviceTallies tallies_from(const mcpet_tallies* out) {
+  DeviceTallies O;
+  memset(&O, 0, sizeof(O));
+  O.trues = out->trues;
+  O.scatter = out->scatter;
+  O.image_trues = out->image_trues;
+  O.image_scatter = out->image_scatter;
+  O.spectrum = out->spectrum;
+  O.psf = (uint32_t*)out->psf;
+  O.psf_count = out->psf_count;
+  O.histories = out->total_histories;
+  O.coincidences = out->coincidences;
+  O.counters = (unsigned long long*)out->counters;
+  return O;
 }
 
 extern "C" {
@@ -643,36 +910,69 @@ mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallie
   double ms = 0;
   s = enqueue_run(sc, opts, O, st, &ms);
   if (s != MCPET_OK) return s;
-  CUDA_TRY(cudaStreamSynchronize(st));
-  const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
-  if (out->trues) CUDA_TRY(cudaMemcpyAsync(out->trues, d.trues, nb, cudaMemcpyDeviceToHost, st));
-  if (out->scatter) CUDA_TRY(cudaMemcpyAsync(out->scatter, d.scatter, nb, cudaMemcpyDeviceToHost, st));
-  if (out->image_trues) CUDA_TRY(cudaMemcpyAsync(out->image_trues, d.img_t, nv, cudaMemcpyDeviceToHost, st));
-  if (out->image_scatter) CUDA_TRY(cudaMemcpyAsync(out->image_scatter, d.img_s, nv, cudaMemcpyDeviceToHost, st));
-  if (out->spectrum)
-    CUDA_TRY(cudaMemcpyAsync(out->spectrum, d.spectrum, (size_t)sc->cfg.n_energy_bins * 4, cudaMemcpyDeviceToHost,
-                             st));
-  unsigned long long small[16];
-  CUDA_TRY(cudaMemcpyAsync(small, d.small, sizeof(small), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  int psf_count = (int)(small[3] & 0xffffffffull);
-  if (out->psf_count) *out->psf_count = psf_count;
-  if (out->total_histories) *out->total_histories = small[2];
-  if (out->coincidences) *out->coincidences = small[14];
-  if (want_psf) {
-    long long n = std::min<long long>(std::max(psf_count, 0), std::min<long long>(d.psf_cap, out->psf_capacity));
-    if (n > 0) CUDA_TRY(cudaMemcpy(out->psf, d.psf, (size_t)n * 44, cudaMemcpyDeviceToHost));
+  return download_run(sc, opts, out, want_psf, ms, st);
+}
+
+mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                                    mcpet_tallies* device_outs) {
+  mcpet_status cs = check_batch(scenes, n_scenes, opts, nullptr);
+  if (cs != MCPET_OK) return cs;
+  if (!device_outs) return set_error(MCPET_ERR_ARG, "null argument");
+  std::vector<DeviceTallies> O((size_t)n_scenes);
+  for (int k = 0; k < n_scenes; ++k) O[(size_t)k] = tallies_from(&device_outs[k]);
+  cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
+  double ms = 0;
+  mcpet_status s = enqueue_batch(scenes, n_scenes, opts, O.data(), st, device_outs[0].transport_ms ? &ms : nullptr);
+  if (s == MCPET_OK && device_outs[0].transport_ms) *device_outs[0].transport_ms = ms;
+  return s;
+}
+
+mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                             mcpet_tallies* outs) {
+  mcpet_status cs = check_batch(scenes, n_scenes, opts, nullptr);
+  if (cs != MCPET_OK) return cs;
+  if (!outs) return set_error(MCPET_ERR_ARG, "null argument");
+  std::vector<DeviceTallies> O((size_t)n_scenes);
+  std::vector<char> want((size_t)n_scenes, 0);
+  for (int k = 0; k < n_scenes; ++k) {
+    mcpet_scene* sc = scenes[k];
+    mcpet_status s = (k > 0 && sc->dev.device < 0) ? mcpet_scene_to_device(sc, scenes[0]->dev.device) : ensure_device(sc);
+    if (s != MCPET_OK) return s;
+    s = upload_tables(sc);
+    if (s != MCPET_OK) return s;
+    const bool want_psf = (sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 1) && outs[k].psf;
+    want[(size_t)k] = want_psf;
+    s = ensure_run_buffers(sc, want_psf);
+    if (s != MCPET_OK) return s;
+    auto& d = sc->dev;
+    DeviceTallies& z = O[(size_t)k];
+    memset(&z, 0, sizeof(z));
+    z.trues = d.trues;
+    z.scatter = d.scatter;
+    z.image_trues = d.img_t;
+    z.image_scatter = d.img_s;
+    z.spectrum = d.spectrum;
+    z.psf = want_psf ? d.psf : nullptr;
+    z.histories = d.small + 2;
+    z.psf_count = (int*)(d.small + 3);
+    z.coincidences = d.small + 14;
+    z.counters = (k == 0 && opts && opts->collect_counters) ? d.small + 4 : nullptr;
   }
-  if (out->counters) {
-    memset(out->counters, 0, sizeof(mcpet_counters));
-    if (opts && opts->collect_counters) memcpy(out->counters, small + 4, 10 * 8);
-    out->counters->guard_trips = small[0];
+  cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
+  double ms = 0;
+  mcpet_status s = enqueue_batch(scenes, n_scenes, opts, O.data(), st, &ms);
+  if (s != MCPET_OK) return s;
+  /* scene 0 holds the launch's guard word and counters */
+  mcpet_run_opts rest;
+  memset(&rest, 0, sizeof(rest));
+  if (opts) rest = *opts;
+  rest.collect_counters = 0;
+  mcpet_status err = MCPET_OK;
+  for (int k = 0; k < n_scenes; ++k) {
+    s = download_run(scenes[k], k == 0 ? opts : &rest, &outs[k], want[(size_t)k] != 0, ms, st);
+    if (s != MCPET_OK && err == MCPET_OK) err = s;
   }
-  if (out->transport_ms) *out->transport_ms = ms;
-  d.last_guard = small[0];
-  if (small[0] != 0)
-    return set_error(MCPET_ERR_DEVICE, "%llu device guard(s) fired (loop cap or out-of-range index)", small[0]);
-  return MCPET_OK;
+  return err;
 }
 
 mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_device, const mcpet_run_opts* opts,

@@ -258,7 +258,14 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
       float ea = a.energy + (P.e_resol * (1.0f / 2.35f)) * a.energy * g2;
       if (fabsf(za) < 0.5f * P.height && (eb > P.e_low) && (eb < P.e_high) && (ea > P.e_low) &&
           (ea < P.e_high)) {
-        int k = atomicAdd(O.psf_count, 2);
+        /* one counter atomic per converged group of lanes, 2 records per lane */
+        const unsigned grp = __activemask();
+        const int leader = __ffs(grp) - 1;
+        const int lane_id = (int)(threadIdx.x & 31);
+        int base = 0;
+        if (lane_id == leader) base = atomicAdd(O.psf_count, 2 * __popc(grp));
+        base = __shfl_sync(grp, base, leader);
+        const int k = base + 2 * __popc(grp & ((1u << lane_id) - 1u));
         if (k > 2000000000) *O.psf_count = 2000000000;
         if (k < P.psf_capacity - 1 && O.psf) {
           long long kb = (travel_b < travel_a) ? k : k + 1;
@@ -425,9 +432,17 @@ struct ColdState {
 };
 
 
-template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false>
+template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false, bool kBatch = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(TransportParams P, DeviceTables T,
-                                                                              DeviceTallies O) {
+                                                                              DeviceTallies O,
+                                                                              const SceneSlot* __restrict__ slots,
+                                                                              int n_slots) {
+  /* kBatch: the lanes belong to n_slots scenes.  P, T and O then describe
+   * the launch (total lanes, work queue, guard word, counters, the Compton
+   * and Rayleigh tables of all scenes' materials; shared staging off); the
+   * launch's lanes are the scenes' lanes one scene after the other, and each
+   * lane reads its scene's parameters, lane plan, tables and tallies from
+   * slots[scene]. */
   /* kDevicePlan: the lane plan was built on the device and its size is read
    * from device memory instead of the launch parameters */
   const uint64_t n_lanes = kDevicePlan ? (uint64_t)O.plan_counts[0] : P.n_lanes;
@@ -468,7 +483,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   LaneCounters cnt = {};
   unsigned long long histories = 0, detected = 0;
   const bool background = P.background_mode != 0;
-  const float2* wood = reinterpret_cast<const float2*>(T.woodcock);
+  int scene = 0;            /* scene of the current lane (kBatch) */
 
   /* hot per-thread state */
   Rng rng = {0, 0};
@@ -489,12 +504,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   float4 rec_hi = make_float4(0.f, 0.f, 0.f, 0.f);
 
   /* photon emitted at ph.pos with ph.dir: set up its tracking */
-  auto start_photon = [&]() {
+  auto start_photon = [&](const TransportParams& PS, const DeviceTables& TS) {
     ph.energy = kAnnihilation;
     ph.travel = 0.0f;
     ph.state = 0;
-    index = __float2int_rd((ph.energy - P.e0) * P.ide);
-    float2 w = __ldg(wood + index);
+    index = __float2int_rd((ph.energy - PS.e0) * PS.ide);
+    float2 w = __ldg(reinterpret_cast<const float2*>(TS.woodcock) + index);
     mfp_w = w.x + ph.energy * w.y;
     mat_old = -1;
     steps = 0;
@@ -510,6 +525,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
     const unsigned m_cmp = __ballot_sync(0xffffffffu, phase == kPhCompton);
     const unsigned m_end = __ballot_sync(0xffffffffu, phase == kPhEnd);
     if (!(m_dec | m_step | m_cmp | m_end)) break;
+    const TransportParams& PS = kBatch ? slots[scene].P : P;
+    const DeviceTables& TS = kBatch ? slots[scene].T : T;
     /* phase of this round: scattering and pair bookkeeping wait until enough
      * lanes need them; Woodcock steps fill the rest */
     const int n_cmp = __popc(m_cmp), n_pair = __popc(m_end | m_dec);
@@ -540,9 +557,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           rotate(ph.dir, costh, 6.28318530717958647693 * ranecu_double(rng));
           if (is_compton) {
             Counting<kCount>::add(cnt.compton, 1);
-            index = __float2int_rd((e - P.e0) * P.ide);
+            index = __float2int_rd((e - PS.e0) * PS.ide);
             if (index > -1) {
-              float2 w = __ldg(wood + index);
+              float2 w = __ldg(reinterpret_cast<const float2*>(TS.woodcock) + index);
               mfp_w = w.x + e * w.y;
               mat_old = -2;
               ph.state = (ph.state == 0) ? 1 : 3;
@@ -578,7 +595,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           emit_second(rng, background, d0, ph.dir);
           ph.pos = make_float3(cold.f(kCOx), cold.f(kCOy), cold.f(kCOz));
           which = 2;
-          start_photon();
+          start_photon(PS, TS);
         } else {
           const float ea = cold.f(kCAe);
           if (escaped && ea > -0.5f) {
@@ -588,10 +605,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             a.energy = ea;
             a.travel = cold.f(kCAt);
             a.state = (int)cold.u(kCAs);
-            const bool pass = (P.tally_type == 0) || (P.tally_type == 1 && ph.state == 0 && a.state == 0) ||
-                              (P.tally_type == 2 && (ph.state != 0 || a.state != 0));
+            const bool pass = (PS.tally_type == 0) || (PS.tally_type == 1 && ph.state == 0 && a.state == 0) ||
+                              (PS.tally_type == 2 && (ph.state != 0 || a.state != 0));
             if (pass)
-              detect_pair<kCount>(rng, P, O, spec_sh, (int)cold.u(kCVox), cold.t_left(), ph, a, cnt, detected);
+              detect_pair<kCount>(rng, PS, kBatch ? slots[scene].O : O, spec_sh, (int)cold.u(kCVox), cold.t_left(),
+                                  ph, a, cnt, detected);
           }
           phase = kPhDecay;
         }
@@ -600,19 +618,43 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
       if (phase == kPhDecay) {
         for (;;) {
           if (!lane_live) {
+            if (kBatch && (histories | detected)) {
+              /* per-scene totals of the lane that just ended */
+              if (histories) atomicAdd(slots[scene].O.histories, histories);
+              if (detected && slots[scene].O.coincidences) atomicAdd(slots[scene].O.coincidences, detected);
+              histories = 0;
+              detected = 0;
+            }
             const uint64_t lane = claim_lane(O.lane_cursor);
             if (lane >= n_lanes) {
               phase = kPhDone;
               break;
             }
-            const Emitter* em = T.emitters + find_emitter(T.emitters, n_emitters, lane);
-            rng = rng_stream(P, __ldg(&em->stream_base) + (lane - __ldg(&em->first_lane)));
+            uint64_t local = lane;
+            const Emitter* plan = T.emitters;
+            int plan_n = n_emitters;
+            if (kBatch) {
+              int lo = 0, hi = n_slots - 1;   /* last scene whose first lane is <= lane */
+              while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&slots[mid].first_lane) <= lane) lo = mid;
+                else hi = mid - 1;
+              }
+              scene = lo;
+              local = lane - __ldg(&slots[scene].first_lane);
+              plan = slots[scene].T.emitters;
+              plan_n = slots[scene].P.n_emitters;
+            }
+            const Emitter* em = plan + find_emitter(plan, plan_n, local);
+            const TransportParams& PN = kBatch ? slots[scene].P : P;
+            rng = rng_stream(PN, __ldg(&em->stream_base) + (local - __ldg(&em->first_lane)));
             cold.set_inv_rate(__ldg(&em->inv_rate));
-            cold.set_t_left(P.acq_ps);
+            cold.set_t_left(PN.acq_ps);
             cold.u(kCVox) = __ldg(&em->voxel);
             lane_live = true;
             Counting<kCount>::add(cnt.lanes, 1);
           }
+          const TransportParams& PN = kBatch ? slots[scene].P : P;
           double inv_act = cold.inv_rate();
           unsigned long long t_left = cold.t_left();
           double dt = -log(ranecu_double(rng)) * inv_act;
@@ -623,27 +665,27 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           }
           cold.set_t_left(t_left - dt_ps);
           histories += 2;
-          cold.set_inv_rate(inv_act * exp(dt * P.inv_mean_life));
+          cold.set_inv_rate(inv_act * exp(dt * PN.inv_mean_life));
           const int voxel = (int)cold.u(kCVox);
-          emit_first(rng, P, voxel % P.nx, (voxel / P.nx) % P.ny, voxel / (P.nx * P.ny), ph.pos, ph.dir);
+          emit_first(rng, PN, voxel % PN.nx, (voxel / PN.nx) % PN.ny, voxel / (PN.nx * PN.ny), ph.pos, ph.dir);
           cold.setf(kCOx, ph.pos.x); cold.setf(kCOy, ph.pos.y); cold.setf(kCOz, ph.pos.z);
           cold.setf(kCDx, ph.dir.x); cold.setf(kCDy, ph.dir.y); cold.setf(kCDz, ph.dir.z);
           which = 1;
-          start_photon();
+          start_photon(PN, kBatch ? slots[scene].T : T);
           break;
         }
       }
     } else {
       /* ---- Woodcock sub-steps (MCGPU-PET_kernel.cu:313-393), repeated while
-       * at least half of the warp's stepping photons are still stepping */
-      const int quorum = (__popc(m_step) + 1) >> 1;
+       * at least step_keep/8 of the warp's stepping photons still step */
+      const int quorum = (__popc(m_step) * P.step_keep + 7) >> 3;
       for (;;) {
         if (phase == kPhStep) {
           const float E = ph.energy;
           bool go = true;
           if (fresh) {
             fresh = false;
-            if (locate(P, ph.pos.x, ph.pos.y, ph.pos.z) < 0) {
+            if (locate(PS, ph.pos.x, ph.pos.y, ph.pos.z) < 0) {
               escaped = true;
               phase = kPhEnd;
               go = false;
@@ -655,20 +697,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             ph.pos.x += step * ph.dir.x;
             ph.pos.y += step * ph.dir.y;
             ph.pos.z += step * ph.dir.z;
-            const int vox = locate(P, ph.pos.x, ph.pos.y, ph.pos.z);
+            const int vox = locate(PS, ph.pos.x, ph.pos.y, ph.pos.z);
             if (vox < 0) {
               escaped = true;
               phase = kPhEnd;
-            } else if ((unsigned long long)vox >= (unsigned long long)P.n_voxels || ++steps > kMaxWoodcockSteps) {
+            } else if ((unsigned long long)vox >= (unsigned long long)PS.n_voxels || ++steps > kMaxWoodcockSteps) {
               Counting<true>::add(cnt.guard, 1);
               escaped = false;
               phase = kPhEnd;
             } else {
-              const uint32_t key = T.vox16 ? (uint32_t)__ldg(&T.vox16[vox]) : __ldg(&T.vox32[vox]);
-              const PaletteEntry pe = pal[key];
+              const uint32_t key = TS.vox16 ? (uint32_t)__ldg(&TS.vox16[vox]) : __ldg(&TS.vox32[vox]);
+              const PaletteEntry pe = kBatch ? TS.palette[key] : pal[key];
               mat0 = pe.mat0;
               Counting<kCount>::add(cnt.steps, 1);
-              const float2* rec = reinterpret_cast<const float2*>(T.mfp + (size_t)index * kMaxMaterials + mat0);
+              const float2* rec = reinterpret_cast<const float2*>(TS.mfp + (size_t)index * kMaxMaterials + mat0);
               if (mat0 != mat_old) {
                 const float2 ab = __ldg(rec);
                 cax = ab.x;
@@ -709,8 +751,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
     }
   }
 
-  atomicAdd(O.histories, histories);
-  if (detected) atomicAdd(O.coincidences, detected);
+  if (kBatch) {
+    if (histories) atomicAdd(slots[scene].O.histories, histories);
+    if (detected && slots[scene].O.coincidences) atomicAdd(slots[scene].O.coincidences, detected);
+  } else {
+    atomicAdd(O.histories, histories);
+    if (detected) atomicAdd(O.coincidences, detected);
+  }
   if (cnt.guard) atomicAdd(O.guard, cnt.guard);
   if (kCount && O.counters) {
     atomicAdd(&O.counters[0], cnt.steps);
@@ -1059,15 +1106,30 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream) {
   if (algorithm == kAlgorithmEvents) {
-    if (counters) transport_events_kernel<true, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O);
-    else transport_events_kernel<false, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O);
+    if (counters) transport_events_kernel<true, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
+    else transport_events_kernel<false, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   } else if (algorithm == kAlgorithmEventsUncapped) {
-    if (counters) transport_events_kernel<true><<<grid, block, smem, stream>>>(P, T, O);
-    else transport_events_kernel<false><<<grid, block, smem, stream>>>(P, T, O);
+    if (counters) transport_events_kernel<true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
+    else transport_events_kernel<false><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   } else {
     if (counters) transport_kernel<true><<<grid, block, smem, stream>>>(P, T, O);
     else transport_kernel<false><<<grid, block, smem, stream>>>(P, T, O);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t transport_batch_occupancy(bool counters, int block, size_t smem, int* blocks_per_sm) {
+  return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, true>, block, smem, blocks_per_sm)
+                  : occupancy_of(transport_events_kernel<false, kEventBlocks, false, true>, block, smem, blocks_per_sm);
+}
+
+cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
+                                   const SceneSlot* slots, int n_slots, bool counters, int grid, int block,
+                                   size_t smem, cudaStream_t stream) {
+  if (counters)
+    transport_events_kernel<true, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
+  else
+    transport_events_kernel<false, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
   return cudaGetLastError();
 }
 
@@ -1114,10 +1176,10 @@ cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, D
   if (!O.coincidences) O.coincidences = &S->header[4];
   if (counters) {
     e = occupancy_smem_attr(transport_events_kernel<true, kEventBlocks, true>, smem);
-    if (e == cudaSuccess) transport_events_kernel<true, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O);
+    if (e == cudaSuccess) transport_events_kernel<true, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   } else {
     e = occupancy_smem_attr(transport_events_kernel<false, kEventBlocks, true>, smem);
-    if (e == cudaSuccess) transport_events_kernel<false, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O);
+    if (e == cudaSuccess) transport_events_kernel<false, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   }
   if (e != cudaSuccess) return e;
   return cudaGetLastError();

@@ -18,6 +18,12 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream);
 
+/* batched runs: several scenes in one launch of the event kernel */
+cudaError_t transport_batch_occupancy(bool counters, int block, size_t smem, int* blocks_per_sm);
+cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
+                                   const SceneSlot* slots, int n_slots, bool counters, int grid, int block,
+                                   size_t smem, cudaStream_t stream);
+
 /* allocation-free runs: lane plan and work-queue words in a static device array */
 constexpr int kNoAllocMaxVoxels = 1 << 20;
 cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,

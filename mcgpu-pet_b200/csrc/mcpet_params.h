@@ -93,6 +93,7 @@ struct TransportParams {
   float e_annihilation;   /* 510998.95 eV, passed at run time */
   int quorum_scatter;     /* event loop: lanes needed to run a scattering round */
   int quorum_pair;        /* ... and a pair-bookkeeping (end of photon, next decay) round */
+  int step_keep;          /* Woodcock batches continue while step_keep/8 of the stepping lanes step */
 };
 
 /* Device pointers of one scene (all read-only during transport). */
@@ -123,6 +124,16 @@ struct DeviceTallies {
   unsigned long long* guard;      /* guard trips */
   unsigned long long* lane_cursor;/* lane work queue head */
   const unsigned long long* plan_counts; /* [lanes, emitters] on the device (device-built plans) */
+};
+
+/* One scene of a batched launch: its parameters (P.n_lanes, P.n_emitters:
+ * its own lane plan T.emitters), tables and outputs, and the first lane of
+ * the launch that belongs to it. */
+struct SceneSlot {
+  TransportParams P;
+  DeviceTables T;
+  DeviceTallies O;
+  unsigned long long first_lane;
 };
 
 }  // namespace mcpet

@@ -163,6 +163,8 @@ _SIGNATURES = {
     "mcpet_scene_to_device": (C.c_int, [P, C.c_int]),
     "mcpet_run": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_device": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
+    "mcpet_run_batch": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
+    "mcpet_run_batch_device": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_device_noalloc": (C.c_int, [P, P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_last_run_guard": (C.c_int, [P, C.POINTER(C.c_ulonglong)]),
     "mcpet_write_outputs": (C.c_int, [P, C.POINTER(Tallies), C.c_char_p, C.c_int, C.c_double]),

@@ -278,6 +278,26 @@ def scanner_for_head() -> dict:
                 n_radial=256, n_z_slices=127, max_ring_difference=63, span=1)
 
 
+def scanner_batch() -> dict:
+    """41 cm radius, 32 rings x 4 mm, 128x128 sinograms (256 crystals), span 1,
+    MRD 31: the scanner of the batched many-phantom workload."""
+    return dict(detector_radius=-41.0, detector_height=12.8, fov_z=12.8, n_rows=32, n_crystals=256, n_angles=128,
+                n_radial=128, n_z_slices=63, max_ring_difference=31, span=1)
+
+
+def batch_phantoms(n: int, emissions_each: float, seed: int = 3):
+    """n seeded head-like phantoms of m^3 voxels, m drawn in [32, 192], voxel
+    pitch in [2, 4] mm (at most 40 cm across), each with emissions_each
+    decays.  Yields (material, density, activity, voxel_size, tissues)."""
+    rng = np.random.default_rng(seed)
+    for k in range(n):
+        m = int(rng.integers(32, 193))
+        vox = float(min(rng.uniform(0.2, 0.4), 40.0 / m))
+        mat, rho, act, vs, used = head_phantom(shape=(m, m, m), voxel_cm=vox, seed=seed * 1000 + k,
+                                               total_bq=emissions_each)
+        yield mat, rho, act, vs, used
+
+
 def scanner_small() -> dict:
     """40 cm radius, 20 cm axial, 15 rings, 147 radial x 168 angles, span 1."""
     return dict(detector_radius=-40.0, detector_height=20.0, fov_z=20.0, n_rows=15, n_crystals=336, n_angles=168,

@@ -97,6 +97,47 @@ def read_config(in_path: str) -> _abi.Config:
     return cfg
 
 
+class _HostRun:
+    """Host (numpy) buffers of one run and the mcpet_tallies pointing at them."""
+
+    def __init__(self, scene: "Scene", psf_capacity: Optional[int]):
+        cfg, info = scene.config, scene.info
+        sino = cfg.tally_psf_sinogram in (0, 2)
+        want_psf = cfg.tally_psf_sinogram in (0, 1)
+        nb, nv = int(cfg.n_bins), int(info.n_voxels)
+        self.trues = np.zeros(nb, np.int32) if sino else None
+        self.scatter = np.zeros(nb, np.int32) if sino else None
+        self.img_t = np.zeros(nv, np.int32) if sino else None
+        self.img_s = np.zeros(nv, np.int32) if sino else None
+        self.spec = np.zeros(max(cfg.n_energy_bins, 1), np.int32)
+        self.cap = int(cfg.psf_size if psf_capacity is None else psf_capacity) if want_psf else 0
+        self.psf = np.zeros(self.cap, PSF_DTYPE) if self.cap > 0 else None
+        self.psf_count = C.c_int32(0)
+        self.hist = C.c_ulonglong(0)
+        self.det = C.c_ulonglong(0)
+        self.ms = C.c_double(0)
+        self.cnt = _abi.Counters()
+        t = _abi.Tallies()
+        t.trues, t.scatter = _ptr(self.trues), _ptr(self.scatter)
+        t.image_trues, t.image_scatter = _ptr(self.img_t), _ptr(self.img_s)
+        t.spectrum = _ptr(self.spec)
+        t.psf = _ptr(self.psf) if self.psf is not None else None
+        t.psf_capacity = self.cap
+        t.psf_count = C.addressof(self.psf_count)
+        t.total_histories = C.addressof(self.hist)
+        t.coincidences = C.addressof(self.det)
+        t.counters = C.addressof(self.cnt)
+        t.transport_ms = C.addressof(self.ms)
+        self.t = t
+
+    def result(self) -> RunResult:
+        n = self.psf_count.value
+        counters = {name: int(getattr(self.cnt, name)) for name, _ in _abi.Counters._fields_}
+        psf = self.psf[: max(0, min(n, self.cap))] if self.psf is not None else None
+        return RunResult(self.trues, self.scatter, self.img_t, self.img_s, self.spec, psf, n, int(self.hist.value),
+                         float(self.ms.value), counters, int(self.det.value))
+
+
 class Scene:
     """A loaded phantom + material tables (+ its device copy)."""
 
@@ -194,42 +235,31 @@ class Scene:
     def to_device(self, device: int = -1) -> None:
         check(lib().mcpet_scene_to_device(self._h, device))
 
+    def _host_run(self, psf_capacity: Optional[int] = None) -> "_HostRun":
+        return _HostRun(self, psf_capacity)
+
     def run(self, opts: Optional[RunOptions] = None, psf_capacity: Optional[int] = None) -> RunResult:
         """End-to-end run into host (numpy) buffers (mcpet_run)."""
         opts = opts or RunOptions()
-        cfg, info = self.config, self.info
-        sino = cfg.tally_psf_sinogram in (0, 2)
-        want_psf = cfg.tally_psf_sinogram in (0, 1)
-        nb, nv = int(cfg.n_bins), int(info.n_voxels)
-        trues = np.zeros(nb, np.int32) if sino else None
-        scatter = np.zeros(nb, np.int32) if sino else None
-        img_t = np.zeros(nv, np.int32) if sino else None
-        img_s = np.zeros(nv, np.int32) if sino else None
-        spec = np.zeros(max(cfg.n_energy_bins, 1), np.int32)
-        cap = int(cfg.psf_size if psf_capacity is None else psf_capacity) if want_psf else 0
-        psf = np.zeros(cap, PSF_DTYPE) if cap > 0 else None
-        psf_count = C.c_int32(0)
-        hist = C.c_ulonglong(0)
-        det = C.c_ulonglong(0)
-        ms = C.c_double(0)
-        cnt = _abi.Counters()
-        t = _abi.Tallies()
-        t.trues, t.scatter, t.image_trues, t.image_scatter = _ptr(trues), _ptr(scatter), _ptr(img_t), _ptr(img_s)
-        t.spectrum = _ptr(spec)
-        t.psf = _ptr(psf) if psf is not None else None
-        t.psf_capacity = cap
-        t.psf_count = C.addressof(psf_count)
-        t.total_histories = C.addressof(hist)
-        t.coincidences = C.addressof(det)
-        t.counters = C.addressof(cnt)
-        t.transport_ms = C.addressof(ms)
+        h = self._host_run(psf_capacity)
         co = opts.to_c()
-        check(lib().mcpet_run(self._h, C.byref(co), C.byref(t)))
-        n = psf_count.value
-        counters = {name: int(getattr(cnt, name)) for name, _ in _abi.Counters._fields_}
-        return RunResult(trues, scatter, img_t, img_s, spec,
-                         psf[: max(0, min(n, cap))] if psf is not None else None, n, int(hist.value),
-                         float(ms.value), counters, int(det.value))
+        check(lib().mcpet_run(self._h, C.byref(co), C.byref(h.t)))
+        return h.result()
+
+    @staticmethod
+    def run_batch(scenes: list, opts: Optional[RunOptions] = None,
+                  psf_capacity: Optional[int] = None) -> list:
+        """Several scenes in one launch (mcpet_run_batch); one RunResult per
+        scene, each equal to scene.run(opts) on its own.  transport_ms is the
+        time of the whole launch; counters (if requested) are launch totals
+        reported on the first result."""
+        opts = opts or RunOptions()
+        hs = [sc._host_run(psf_capacity) for sc in scenes]
+        arr = (_abi.Tallies * len(hs))(*[h.t for h in hs])
+        ptrs = (C.c_void_p * max(len(scenes), 1))(*[sc._h.value for sc in scenes])
+        co = opts.to_c()
+        check(lib().mcpet_run_batch(ptrs, len(scenes), C.byref(co), arr))
+        return [h.result() for h in hs]
 
     def run_into(self, host: dict, opts: Optional[RunOptions] = None) -> dict:
         """End-to-end run (mcpet_run) writing into caller-provided host buffers
