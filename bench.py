@@ -234,6 +234,49 @@ def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8) ->
             "kernel_speedup": seq_ms / bat_ms, "wall_speedup": seq_wall / bat_wall, "unit": UNIT}
 
 
+def measure_gradient(workdir: str, emissions: float = 2.0e8) -> dict:
+    """Gradient of the sinogram log-likelihood on the head phantom (2e8
+    decays): the measured sinogram is another seed's forward run with grey
+    matter activity x1.5 plus 5 % uniform randoms.  Reports the device time
+    of the gradient call (forward with event records + log-likelihood +
+    replay) against a plain forward run of the same scene."""
+    import torch
+    import mcpet
+    from mcpet import grad as G
+    from mcpet import inputs
+    mat, rho, act, vs, used = inputs.head_phantom(shape=(64, 128, 128), voxel_cm=0.2, seed=PHANTOM_SEED,
+                                                  total_bq=emissions)
+    spec = inputs.spec_for(inputs.tissue_materials(used), "unused.vox", seed=12345, **inputs.scanner_for_head())
+    cfg = inputs.config_from_spec(spec, workdir)
+    act_true = act.copy()
+    act_true[mat == inputs.TISSUES["grey"][0]] *= 1.5
+    sc_t = mcpet.Scene.from_arrays(cfg, mat, rho, act_true, vs)
+    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED, seed_override=777)
+    t = G._device_tallies(sc_t, torch, torch.device("cuda"))
+    sc_t.run_device(t, opts)
+    tot = (t["trues"] + t["scatter"]).to(torch.float32)
+    bg = torch.full_like(tot, 0.05 * float(tot.sum()) / tot.numel())
+    y = tot + torch.poisson(bg)
+    sc_t.close()
+    del t, tot
+    sc = mcpet.Scene.from_arrays(cfg, mat, rho, act, vs)
+    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED)
+    tall = G._device_tallies(sc, torch, torch.device("cuda"))
+    r = G.grad(sc, y, bg, opts, tallies=tall)             # warm-up (event buffer, device activity)
+    plain = [sc.run_device(tall, opts, time_it=True) for _ in range(3)]
+    runs = [G.grad(sc, y, bg, opts, tallies=tall) for _ in range(3)]
+    r = runs[-1]
+    fwd = min(x.forward_ms for x in runs)
+    gms = min(x.gradient_ms for x in runs)
+    sc.close()
+    return {"workload": f"head phantom 128x128x64 @ 2 mm, {emissions:.0e} decays, 64-ring scanner; measured "
+                        "sinogram: another seed with grey-matter activity x1.5 plus 5% uniform randoms",
+            "plain_forward_ms": min(plain), "forward_with_records_ms": fwd, "gradient_pass_ms": gms,
+            "gradient_time_over_forward": (fwd + gms) / min(plain),
+            "events": r.events, "replay_mismatches": r.mismatches, "loglik": r.loglik,
+            "outputs": "dL/dA and dL/ds for every voxel"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -250,6 +293,7 @@ def main():
                     help="also time N phantoms of m^3 voxels (m in [32,192], 1e8 decays each) batched in one "
                          "launch against the same runs one by one (reported under 'batch')")
     ap.add_argument("--batch-emissions", type=float, default=1.0e8, help="decays per phantom of --batch-scenes")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the gradient (mcpet_grad) measurement")
     ap.add_argument("--scanner", default="head", choices=["head", "head32"],
                     help="head32: smaller sinogram for profiler captures (not a bench line)")
     args = ap.parse_args()
@@ -386,6 +430,10 @@ def main():
         except Exception:
             pass
 
+    gradient = None
+    if rank == 0 and world == 1 and not args.no_gradient:
+        gradient = measure_gradient(tmp)
+
     batch = None
     if args.batch_scenes > 0 and rank == 0:
         batch = measure_batch(args.batch_scenes, tmp, args.batch_emissions)
@@ -406,6 +454,8 @@ def main():
                            "coincidences_per_step": total / args.steps / world, "histories_last_step": hist,
                            "guard_trips": guard},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks}
+        if gradient is not None:
+            line["gradient"] = gradient
         if batch is not None:
             line["batch"] = batch
         print(json.dumps(line))

@@ -238,6 +238,37 @@ mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
 mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                              mcpet_tallies* outs);
 
+/* Gradient of the Poisson log-likelihood of a measured sinogram,
+ *   L = sum_b y_b ln(lambda_b) - lambda_b,  lambda = trues + scatter + background,
+ * with respect to each voxel's activity and density scale.  No counterpart
+ * in the reference (it has no adjoint); the forward model is its transport
+ * (mcpet_run_device on device_out, same options and results).  Activity:
+ * event back-tallying of w_b = y_b/lambda_b - 1 over the tallied
+ * coincidences, divided by the voxel activity.  Density scale s_v (rho_v ->
+ * s_v rho_v, majorant held fixed): path-replay score function -- every
+ * tallied history is recomputed from the RANECU state recorded at its
+ * emission and each Woodcock step inside a voxel adds w_b times
+ * d ln p(step)/d ln rho to it.  A replay that does not reproduce the recorded
+ * bin is left out of dL/ds and counted in mismatches.  Blocking. */
+typedef struct {
+  const float* measured;          /* device [n_bins]: y, the measured sinogram (counts) */
+  const float* background;        /* device [n_bins]: r, expected background added to the model; NULL = 0 */
+  float* grad_activity;           /* device [n_voxels] out: dL/dA_v (per Bq); NULL to skip */
+  float* grad_density_scale;      /* device [n_voxels] out: dL/ds_v; NULL to skip */
+  void* event_buffer;             /* device scratch, 24 bytes per tallied coincidence; NULL: the scene
+                                     keeps one (grown and the forward repeated when too small) */
+  long long event_capacity;       /* records event_buffer holds */
+  double loglik;                  /* out: L */
+  unsigned long long events;      /* out: tallied coincidences of the forward run */
+  unsigned long long replayed;    /* out: replays that reproduced their bin */
+  unsigned long long mismatches;  /* out: replays that did not (left out) */
+  double forward_ms;              /* out: device time of the forward transport (with event records) */
+  double gradient_ms;             /* out: device time of the log-likelihood and the replay */
+} mcpet_grad_args;
+
+mcpet_status mcpet_grad(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_tallies* device_out,
+                        mcpet_grad_args* args);
+
 /* Batched run into DEVICE tallies (device_outs[k] as in mcpet_run_device),
  * ordered on opts->stream; the merged lane plan is uploaded and released in
  * stream order. */

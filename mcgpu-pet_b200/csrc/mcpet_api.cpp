@@ -390,6 +390,7 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   const int block = pick_block(o);
   int algorithm = o.algorithm == kAlgorithmHistories ? kAlgorithmHistories : kAlgorithmEvents;
   if (algorithm == kAlgorithmEvents && env_int("MCPET_MINBLOCKS", 4, 1, 4) == 1) algorithm = kAlgorithmEventsUncapped;
+  if (O.events && algorithm != kAlgorithmHistories) algorithm = kAlgorithmEventsRecord;
   size_t smem = transport_dynamic_smem(P, block, algorithm);
   int bps = 0;
   CUDA_TRY(transport_occupancy(counters, algorithm, block, smem, &bps));
@@ -462,6 +463,9 @@ mcpet_scene::~mcpet_scene() {
     dfree(dev.spectrum);
     dfree(dev.psf);
     dfree(dev.small);
+    dfree(dev.events);
+    dfree(dev.activity);
+    dfree(dev.gwords);
     if (dev.ev0) cudaEventDestroy((cudaEvent_t)dev.ev0);
     if (dev.ev1) cudaEventDestroy((cudaEvent_t)dev.ev1);
   }
@@ -973,6 +977,103 @@ mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcp
     if (s != MCPET_OK && err == MCPET_OK) err = s;
   }
   return err;
+}
+
+mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* device_out,
+                        mcpet_grad_args* g) {
+  if (!sc || !device_out || !g) return set_error(MCPET_ERR_ARG, "null argument");
+  if (!g->measured) return set_error(MCPET_ERR_ARG, "the measured sinogram is required");
+  if (!device_out->trues || !device_out->scatter)
+    return set_error(MCPET_ERR_ARG, "the gradient needs the trues and scatter sinograms of the forward run");
+  if (!(sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 2))
+    return set_error(MCPET_ERR_ARG, "the gradient needs the sinogram tally (REPORT PSF/SINOGRAM 0 or 2)");
+  if (g->event_buffer && g->event_capacity <= 0) return set_error(MCPET_ERR_ARG, "event_capacity must be > 0");
+  mcpet_status s = validate_opts(sc, opts);
+  if (s != MCPET_OK) return s;
+  s = ensure_device(sc);
+  if (s != MCPET_OK) return s;
+  s = upload_tables(sc);
+  if (s != MCPET_OK) return s;
+  auto& d = sc->dev;
+  cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
+  const long long nv = (long long)sc->mat0.size();
+  if (!d.gwords) CUDA_TRY(dmalloc(&d.gwords, 4 * sizeof(unsigned long long)));
+  if (!d.activity) CUDA_TRY(dmalloc(&d.activity, (size_t)nv * sizeof(float)));
+  CUDA_TRY(cudaMemcpyAsync(d.activity, sc->activity.data(), (size_t)nv * sizeof(float), cudaMemcpyHostToDevice, st));
+
+  /* forward transport with event records; grown and repeated (same seed,
+   * same events) if the buffer was too small */
+  unsigned long long n_events = 0;
+  double fwd_ms = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    uint32_t* ev = (uint32_t*)g->event_buffer;
+    long long cap = g->event_capacity;
+    if (!ev) {
+      if (d.event_cap <= 0) {
+        double expect = 0, T = (double)sc->cfg.acquisition_time_ps * 1e-12;
+        for (float a : sc->activity)
+          if (a > 1.0e-7f) expect += (double)a * T;
+        long long want = (long long)std::min(std::max(expect * 0.15, 1.0e6), 2.0e9);
+        CUDA_TRY(dmalloc(&d.events, (size_t)want * sizeof(EventRecord)));
+        d.event_cap = want;
+      }
+      ev = d.events;
+      cap = d.event_cap;
+    }
+    DeviceTallies O = tallies_from(device_out);
+    O.events = ev;
+    O.event_count = d.small + 15;
+    O.event_capacity = cap;
+    CUDA_TRY(cudaMemsetAsync(O.event_count, 0, sizeof(unsigned long long), st));
+    s = enqueue_run(sc, opts, O, st, &fwd_ms);
+    if (s != MCPET_OK) return s;
+    CUDA_TRY(cudaMemcpyAsync(&n_events, d.small + 15, sizeof(n_events), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (n_events <= (unsigned long long)cap) break;
+    if (g->event_buffer || attempt == 1)
+      return set_error(MCPET_ERR_LIMIT, "%llu tallied coincidences, event buffer holds %lld", n_events, cap);
+    dfree(d.events);
+    const long long want = (long long)((double)n_events * 1.1) + 1024;
+    CUDA_TRY(dmalloc(&d.events, (size_t)want * sizeof(EventRecord)));
+    d.event_cap = want;
+  }
+  unsigned long long guard = 0;
+  CUDA_TRY(cudaMemcpy(&guard, d.small, sizeof(guard), cudaMemcpyDeviceToHost));
+  d.last_guard = guard;
+  if (guard != 0)
+    return set_error(MCPET_ERR_DEVICE, "%llu device guard(s) fired (loop cap or out-of-range index)", guard);
+
+  /* log-likelihood and the replay of the recorded events */
+  TransportParams P;
+  fill_params(sc, P);
+  if (opts && opts->seed_override != 0) P.seed = opts->seed_override;
+  P.background_mode = (opts && opts->background_mode) ? 1 : 0;
+  DeviceTables T = device_tables(sc);
+  CUDA_TRY(cudaMemsetAsync(d.gwords, 0, 4 * sizeof(unsigned long long), st));
+  if (g->grad_activity) CUDA_TRY(cudaMemsetAsync(g->grad_activity, 0, (size_t)nv * sizeof(float), st));
+  if (g->grad_density_scale) CUDA_TRY(cudaMemsetAsync(g->grad_density_scale, 0, (size_t)nv * sizeof(float), st));
+  CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
+  CUDA_TRY(launch_loglik(sc->cfg.n_bins, g->measured, device_out->trues, device_out->scatter, g->background,
+                         reinterpret_cast<double*>(d.gwords + 2), d.sm_count, st));
+  if (n_events > 0 && (g->grad_activity || g->grad_density_scale))
+    CUDA_TRY(launch_grad_replay(P, T, g->event_buffer ? (const uint32_t*)g->event_buffer : d.events, n_events,
+                                g->measured, device_out->trues, device_out->scatter, g->background, d.activity,
+                                g->grad_activity, g->grad_density_scale, d.gwords, d.sm_count, st));
+  CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
+  unsigned long long words[4];
+  CUDA_TRY(cudaMemcpyAsync(words, d.gwords, sizeof(words), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  float gms = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&gms, (cudaEvent_t)d.ev0, (cudaEvent_t)d.ev1));
+  double ll;
+  memcpy(&ll, &words[2], sizeof(ll));
+  g->loglik = ll;
+  g->events = n_events;
+  g->replayed = words[0];
+  g->mismatches = words[1];
+  g->forward_ms = fwd_ms;
+  g->gradient_ms = gms;
+  return MCPET_OK;
 }
 
 mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_device, const mcpet_run_opts* opts,

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "mcpet_device.cuh"
@@ -73,13 +74,19 @@ struct PhotonState {
   int state;    /* 0 unscattered, 1 Compton, 2 Rayleigh, 3 multiple */
 };
 
+/* Observer of the Woodcock steps inside the phantom: voxel, whether the
+ * step ended in a real interaction, and the probability of a virtual one. */
+struct NoStepHook {
+  __device__ __forceinline__ void operator()(int, bool, float) {}
+};
+
 /* Transport one photon from its emission point until it leaves the voxel box
  * (returns true) or is absorbed (returns false).  Woodcock delta tracking and
  * interaction selection of MCGPU-PET_kernel.cu:298-414. */
-template <bool kCount, typename Scratch>
+template <bool kCount, typename Scratch, typename Hook = NoStepHook>
 __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P, const DeviceTables& T,
                                              const PaletteEntry* pal, const ComptonTable& C, Scratch rn,
-                                             PhotonState& ph, LaneCounters& cnt) {
+                                             PhotonState& ph, LaneCounters& cnt, Hook* hook = nullptr) {
   float energy = ph.energy;
   int index = __float2int_rd((energy - P.e0) * P.ide);
   float2 w = __ldg(reinterpret_cast<const float2*>(T.woodcock) + index);
@@ -120,6 +127,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       mfp_density = mfp_w * pe.rho;
       prob = 1.0f - mfp_density * (rec_lo.x + energy * rec_lo.y);
       randno = ranecu(rng);
+      if (hook) (*hook)(vox, !(randno < prob), prob);
     } while (randno < prob);
     if (vox < 0) break;
 
@@ -190,11 +198,11 @@ __device__ __forceinline__ void put_psf_record(uint32_t* psf, long long k, unsig
  * (MCGPU-PET_kernel.cu:417-432): sinogram tally (tally_Sinogram,
  * :1624-1836) and/or phase-space tally (tally_PSF_coincidences, :531-644).
  * "b" = the second photon (tracked last), "a" = the first. */
-template <bool kCount>
+template <bool kCount, bool kRecord = true>
 __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, const DeviceTallies& O,
                                             int* spec_sh, int voxel, unsigned long long t_left,
                                             const PhotonState& b, const PhotonState& a, LaneCounters& cnt,
-                                            unsigned long long& detected) {
+                                            unsigned long long& detected, int2 rng_emit) {
   const bool want_sino = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 2);
   const bool want_psf = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 1);
   if (want_sino) {
@@ -234,6 +242,30 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
               }
               detected += 1;
               Counting<kCount>::add(cnt.tallies, 2);
+              if (kRecord && O.events) {
+                /* record for the gradient replay: one counter atomic per
+                 * converged group of lanes */
+                const unsigned grp = __activemask();
+                const int leader = __ffs(grp) - 1;
+                const int lane_id = (int)(threadIdx.x & 31);
+                unsigned long long base = 0;
+                if (lane_id == leader) base = atomicAdd(O.event_count, (unsigned long long)__popc(grp));
+                base = __shfl_sync(grp, base, leader);
+                const unsigned long long k = base + (unsigned long long)__popc(grp & ((1u << lane_id) - 1u));
+                if (k < (unsigned long long)O.event_capacity) {
+                  uint4* rec = reinterpret_cast<uint4*>(O.events + 6 * k);
+                  uint2* rec2 = reinterpret_cast<uint2*>(O.events + 6 * k + 4);
+                  if ((k & 1) == 0) {
+                    rec[0] = make_uint4((uint32_t)rng_emit.x, (uint32_t)rng_emit.y, (uint32_t)voxel, 0u);
+                    rec2[0] = make_uint2((uint32_t)bin, (uint32_t)((unsigned long long)bin >> 32));
+                  } else {
+                    uint2* r = reinterpret_cast<uint2*>(O.events + 6 * k);
+                    r[0] = make_uint2((uint32_t)rng_emit.x, (uint32_t)rng_emit.y);
+                    r[1] = make_uint2((uint32_t)voxel, 0u);
+                    r[2] = make_uint2((uint32_t)bin, (uint32_t)((unsigned long long)bin >> 32));
+                  }
+                }
+              }
             } else {
               Counting<true>::add(cnt.guard, 1);
             }
@@ -339,6 +371,7 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       inv_act = inv_act * exp(dt * P.inv_mean_life);
 
       PhotonState a, b;
+      const int2 rng_emit = make_int2(rng.x, rng.y);
       emit_first(rng, P, vx, vy, vz, a.pos, a.dir);
       const float3 origin = a.pos, dir0 = a.dir;
       a.energy = kAnnihilation;
@@ -357,7 +390,7 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       if (esc_a && esc_b) {
         bool pass = (P.tally_type == 0) || (P.tally_type == 1 && b.state == 0 && a.state == 0) ||
                     (P.tally_type == 2 && (b.state != 0 || a.state != 0));
-        if (pass) detect_pair<kCount>(rng, P, O, spec_sh, voxel, t_left, b, a, cnt, detected);
+        if (pass) detect_pair<kCount>(rng, P, O, spec_sh, voxel, t_left, b, a, cnt, detected, rng_emit);
       }
     }
   }
@@ -406,6 +439,7 @@ enum : int {
   kCAx, kCAy, kCAz, kCAu, kCAv, kCAw,            /* photon 1 at exit: position, direction */
   kCAe, kCAt, kCAs,                              /* photon 1 energy (-10 absorbed), travel, state */
   kCInvLo, kCInvHi, kCTLo, kCTHi, kCVox,         /* lane: 1/rate (double), remaining ps (u64), voxel */
+  kCRx, kCRy,                                    /* RANECU state right before the pair's emission */
   kCold
 };
 
@@ -432,7 +466,7 @@ struct ColdState {
 };
 
 
-template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false, bool kBatch = false>
+template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false, bool kBatch = false, bool kRecord = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(TransportParams P, DeviceTables T,
                                                                               DeviceTallies O,
                                                                               const SceneSlot* __restrict__ slots,
@@ -442,7 +476,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
    * and Rayleigh tables of all scenes' materials; shared staging off); the
    * launch's lanes are the scenes' lanes one scene after the other, and each
    * lane reads its scene's parameters, lane plan, tables and tallies from
-   * slots[scene]. */
+   * slots[scene].  kRecord: tallied coincidences are also written to
+   * O.events for the gradient replay. */
   /* kDevicePlan: the lane plan was built on the device and its size is read
    * from device memory instead of the launch parameters */
   const uint64_t n_lanes = kDevicePlan ? (uint64_t)O.plan_counts[0] : P.n_lanes;
@@ -608,8 +643,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             const bool pass = (PS.tally_type == 0) || (PS.tally_type == 1 && ph.state == 0 && a.state == 0) ||
                               (PS.tally_type == 2 && (ph.state != 0 || a.state != 0));
             if (pass)
-              detect_pair<kCount>(rng, PS, kBatch ? slots[scene].O : O, spec_sh, (int)cold.u(kCVox), cold.t_left(),
-                                  ph, a, cnt, detected);
+              detect_pair<kCount, kRecord>(rng, PS, kBatch ? slots[scene].O : O, spec_sh, (int)cold.u(kCVox),
+                                           cold.t_left(), ph, a, cnt, detected,
+                                           kRecord ? make_int2((int)cold.u(kCRx), (int)cold.u(kCRy))
+                                                   : make_int2(0, 0));
           }
           phase = kPhDecay;
         }
@@ -667,6 +704,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           histories += 2;
           cold.set_inv_rate(inv_act * exp(dt * PN.inv_mean_life));
           const int voxel = (int)cold.u(kCVox);
+          if (kRecord) {
+            cold.u(kCRx) = (uint32_t)rng.x;
+            cold.u(kCRy) = (uint32_t)rng.y;
+          }
           emit_first(rng, PN, voxel % PN.nx, (voxel / PN.nx) % PN.ny, voxel / (PN.nx * PN.ny), ph.pos, ph.dir);
           cold.setf(kCOx, ph.pos.x); cold.setf(kCOy, ph.pos.y); cold.setf(kCOz, ph.pos.z);
           cold.setf(kCDx, ph.dir.x); cold.setf(kCDy, ph.dir.y); cold.setf(kCDz, ph.dir.z);
@@ -885,6 +926,136 @@ __global__ void probe_source_kernel(TransportParams P, int background, int2* see
   seeds[v] = make_int2(r.x, r.y);
 }
 
+/* ------------------------------------------------------ gradient
+ *
+ * The Poisson log-likelihood of a measured sinogram y under the model
+ * lambda = trues + scatter (the forward transport) + background r:
+ *   L = sum_b  y_b ln(lambda_b) - lambda_b.
+ * Its gradient with respect to the voxel activities and density scales is
+ * estimated from the tallied coincidences of the forward run, which recorded
+ * for each one the RANECU state at its emission, its voxel and its bin
+ * (EventRecord).  With w_b = y_b / lambda_b - 1:
+ *   dL/dA_v = sum over events e from voxel v of w_b(e) / A_v
+ * (event back-tallying: lambda is linear in A), and
+ *   dL/ds_v = sum over events e of w_b(e) * S_v(e)
+ * (path-replay score function): S_v(e) sums, over the Woodcock steps of the
+ * event's two photons inside voxel v, d ln p(step) / d ln rho_v -- +1 for a
+ * real interaction, -p_real/(1-p_real) for a virtual one (the majorant is
+ * held fixed; the interaction type and everything after it do not depend on
+ * rho_v).  Each history is recomputed from its RNG state instead of being
+ * stored; a replay whose photons do not land in the recorded bin is counted
+ * and left out of dL/ds (dL/dA needs no replay). */
+
+constexpr int kReplaySteps = 96;   /* voxel runs one replayed pair may visit */
+
+struct ScoreList {
+  int vox[kReplaySteps];
+  float score[kReplaySteps];
+  int n;
+  bool overflow;
+  __device__ __forceinline__ void operator()(int v, bool real, float prob_virtual) {
+    const float sc = real ? 1.0f : (prob_virtual > 0.0f ? -(1.0f - prob_virtual) / prob_virtual : 0.0f);
+    if (n > 0 && vox[n - 1] == v) {
+      score[n - 1] += sc;
+    } else if (n < kReplaySteps) {
+      vox[n] = v;
+      score[n] = sc;
+      ++n;
+    } else {
+      overflow = true;
+    }
+  }
+};
+
+__global__ void __launch_bounds__(kBlock) grad_replay_kernel(TransportParams P, DeviceTables T, const uint32_t* events,
+                                                             unsigned long long n_events, const float* y,
+                                                             const int* trues, const int* scatter, const float* bg,
+                                                             const float* activity, float* grad_a, float* grad_s,
+                                                             unsigned long long* stats) {
+  __shared__ ComptonTable cmp;
+  extern __shared__ float4 dyn_smem[];
+  float* scratch = reinterpret_cast<float*>(dyn_smem);
+  {
+    const int* src = reinterpret_cast<const int*>(T.compton);
+    int* dst = reinterpret_cast<int*>(&cmp);
+    for (int i = threadIdx.x; i < (int)(sizeof(ComptonTable) / 4); i += blockDim.x) dst[i] = __ldg(&src[i]);
+  }
+  __syncthreads();
+  SharedScratch rn{scratch + threadIdx.x, (int)blockDim.x};
+  const bool background = P.background_mode != 0;
+  unsigned long long ok_count = 0, bad_count = 0;
+  LaneCounters cnt = {};
+  ScoreList h;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_events;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t* r = events + 6 * i;
+    Rng rng = {(int)r[0], (int)r[1]};
+    const int voxel = (int)r[2];
+    const long long bin = (long long)(((unsigned long long)r[5] << 32) | r[4]);
+    const float lam = (float)(__ldg(&trues[bin]) + __ldg(&scatter[bin])) + (bg ? __ldg(&bg[bin]) : 0.0f);
+    const float w = __ldg(&y[bin]) / lam - 1.0f;
+    if (grad_a) atomicAdd(&grad_a[voxel], w / __ldg(&activity[voxel]));
+    if (!grad_s) continue;
+    h.n = 0;
+    h.overflow = false;
+    PhotonState a, b;
+    emit_first(rng, P, voxel % P.nx, (voxel / P.nx) % P.ny, voxel / (P.nx * P.ny), a.pos, a.dir);
+    const float3 origin = a.pos, dir0 = a.dir;
+    a.energy = kAnnihilation;
+    a.travel = 0.0f;
+    a.state = 0;
+    const bool esc_a = track_photon<false>(rng, P, T, T.palette, cmp, rn, a, cnt, &h);
+    emit_second(rng, background, dir0, b.dir);
+    b.pos = origin;
+    b.energy = kAnnihilation;
+    b.travel = 0.0f;
+    b.state = 0;
+    const bool esc_b = track_photon<false>(rng, P, T, T.palette, cmp, rn, b, cnt, &h);
+    /* the replayed pair must land in the recorded bin (geometry of the
+     * sinogram tally, MCGPU-PET_kernel.cu:1645-1791) */
+    bool ok = esc_a && esc_b && !h.overflow;
+    if (ok) {
+      float xb, yb, zb, xa, ya, za;
+      to_cylinder(P, b.pos, b.dir, xb, yb, zb);
+      const float phib = atan2f(yb, xb);
+      to_cylinder(P, a.pos, a.dir, xa, ya, za);
+      const float phia = atan2f(ya, xa);
+      ok = fabsf(zb) < 0.5f * P.height && fabsf(za) < 0.5f * P.height &&
+           sinogram_bin(P, phib, zb, phia, za) == bin;
+    }
+    if (!ok) {
+      ++bad_count;
+      continue;
+    }
+    ++ok_count;
+    for (int k = 0; k < h.n; ++k) atomicAdd(&grad_s[h.vox[k]], w * h.score[k]);
+  }
+  if (ok_count) atomicAdd(&stats[0], ok_count);
+  if (bad_count) atomicAdd(&stats[1], bad_count);
+}
+
+/* L = sum_b y_b ln(lambda_b) - lambda_b: FP32 partials per thread and per
+ * block, one FP64 atomic per block. */
+__global__ void __launch_bounds__(256) loglik_kernel(long long nbins, const float* y, const int* trues,
+                                                     const int* scatter, const float* bg, double* out) {
+  float acc = 0.0f;
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nbins;
+       b += (long long)gridDim.x * blockDim.x) {
+    const float lam = (float)(trues[b] + scatter[b]) + (bg ? bg[b] : 0.0f);
+    const float yb = y[b];
+    if (lam > 0.0f) acc += (yb > 0.0f ? yb * logf(lam) : 0.0f) - lam;
+  }
+  __shared__ float part[8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+    atomicAdd(out, (double)t);
+  }
+}
+
 /* ------------------------------------------------ allocation-free runs
  *
  * Scratch of mcpet_run_device_noalloc: the lane plan (built on the device
@@ -1093,6 +1264,11 @@ static cudaError_t occupancy_of(K kernel, int block, size_t smem, int* bps) {
 constexpr int kEventBlocks = 4;
 
 cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t smem, int* blocks_per_sm) {
+  if (algorithm == kAlgorithmEventsRecord)
+    return counters
+               ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, false, true>, block, smem, blocks_per_sm)
+               : occupancy_of(transport_events_kernel<false, kEventBlocks, false, false, true>, block, smem,
+                              blocks_per_sm);
   if (algorithm == kAlgorithmEvents)
     return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks>, block, smem, blocks_per_sm)
                     : occupancy_of(transport_events_kernel<false, kEventBlocks>, block, smem, blocks_per_sm);
@@ -1105,7 +1281,13 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t 
 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream) {
-  if (algorithm == kAlgorithmEvents) {
+  if (algorithm == kAlgorithmEventsRecord) {
+    if (counters)
+      transport_events_kernel<true, kEventBlocks, false, false, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
+    else
+      transport_events_kernel<false, kEventBlocks, false, false, true><<<grid, block, smem, stream>>>(P, T, O, nullptr,
+                                                                                                   0);
+  } else if (algorithm == kAlgorithmEvents) {
     if (counters) transport_events_kernel<true, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
     else transport_events_kernel<false, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   } else if (algorithm == kAlgorithmEventsUncapped) {
@@ -1182,6 +1364,32 @@ cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, D
     if (e == cudaSuccess) transport_events_kernel<false, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   }
   if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_replay(const TransportParams& P, const DeviceTables& T, const uint32_t* events,
+                               unsigned long long n_events, const float* y, const int* trues, const int* scatter,
+                               const float* bg, const float* activity, float* grad_a, float* grad_s,
+                               unsigned long long* stats, int sm_count, cudaStream_t stream) {
+  const size_t smem = (size_t)(P.max_shells > 0 ? P.max_shells : 1) * kBlock * sizeof(float);
+  cudaError_t e = occupancy_smem_attr(grad_replay_kernel, smem);
+  if (e != cudaSuccess) return e;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, grad_replay_kernel, kBlock, smem);
+  if (e != cudaSuccess) return e;
+  if (bps < 1) bps = 1;
+  unsigned long long need = (n_events + kBlock - 1) / kBlock;
+  int grid = (int)std::min<unsigned long long>(need > 0 ? need : 1, (unsigned long long)sm_count * bps);
+  grad_replay_kernel<<<grid, kBlock, smem, stream>>>(P, T, events, n_events, y, trues, scatter, bg, activity, grad_a,
+                                                     grad_s, stats);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_loglik(long long nbins, const float* y, const int* trues, const int* scatter, const float* bg,
+                          double* out, int sm_count, cudaStream_t stream) {
+  long long need = (nbins + 255) / 256;
+  int grid = (int)std::min<long long>(need > 0 ? need : 1, (long long)sm_count * 8);
+  loglik_kernel<<<grid, 256, 0, stream>>>(nbins, y, trues, scatter, bg, out);
   return cudaGetLastError();
 }
 

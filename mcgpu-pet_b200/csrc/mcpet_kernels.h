@@ -11,6 +11,7 @@ namespace mcpet {
 constexpr int kAlgorithmHistories = 1;  /* one lane per thread, history after history */
 constexpr int kAlgorithmEvents = 2;     /* warp-regrouped event loop, registers capped for occupancy */
 constexpr int kAlgorithmEventsUncapped = 3; /* same loop, registers not capped (MCPET_MINBLOCKS=1) */
+constexpr int kAlgorithmEventsRecord = 4;   /* event loop that also records tallied coincidences (gradient) */
 
 size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();
@@ -29,6 +30,14 @@ constexpr int kNoAllocMaxVoxels = 1 << 20;
 cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,
                                      const float* activity, int lane_mode, int tpb, int hpl, bool counters,
                                      int grid, int block, size_t smem, cudaStream_t stream);
+
+/* gradient of the sinogram log-likelihood: replay of the recorded events */
+cudaError_t launch_grad_replay(const TransportParams& P, const DeviceTables& T, const uint32_t* events,
+                               unsigned long long n_events, const float* y, const int* trues, const int* scatter,
+                               const float* bg, const float* activity, float* grad_a, float* grad_s,
+                               unsigned long long* stats, int sm_count, cudaStream_t stream);
+cudaError_t launch_loglik(long long nbins, const float* y, const int* trues, const int* scatter, const float* bg,
+                          double* out, int sm_count, cudaStream_t stream);
 
 cudaError_t launch_probe_rng(const TransportParams& P, int n, const int64_t* ids, int ndraw, int2* seeds,
                              float* draws, double* ddraws, cudaStream_t s);

@@ -124,6 +124,18 @@ struct DeviceTallies {
   unsigned long long* guard;      /* guard trips */
   unsigned long long* lane_cursor;/* lane work queue head */
   const unsigned long long* plan_counts; /* [lanes, emitters] on the device (device-built plans) */
+  uint32_t* events;               /* detected-coincidence records (EventRecord) for the gradient, or NULL */
+  unsigned long long* event_count;
+  long long event_capacity;
+};
+
+/* One tallied coincidence, enough to replay its history: the lane's RANECU
+ * state right before the emission, the emitting voxel and the sinogram bin. */
+struct EventRecord {
+  int32_t rng_x, rng_y;
+  uint32_t voxel;
+  uint32_t pad;
+  long long bin;
 };
 
 /* One scene of a batched launch: its parameters (P.n_lanes, P.n_emitters:

@@ -69,6 +69,11 @@ struct mcpet_scene {
     int ne_alloc = -1;
     void* ev0 = nullptr;
     void* ev1 = nullptr;
+    /* gradient (mcpet_grad): event records, device activity, small words */
+    uint32_t* events = nullptr;
+    long long event_cap = 0;
+    float* activity = nullptr;
+    unsigned long long* gwords = nullptr;  /* 0 replayed, 1 mismatches, 2 log-likelihood (double) */
     unsigned long long last_guard = 0;
     long long run_h2d = 0;        /* host->device bytes of the run in progress */
     long long last_h2d = 0;       /* ... and of the last completed run */

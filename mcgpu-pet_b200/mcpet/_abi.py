@@ -150,6 +150,25 @@ class Tallies(C.Structure):
     ]
 
 
+class GradArgs(C.Structure):
+    _fields_ = [
+        ("measured", C.c_void_p),
+        ("background", C.c_void_p),
+        ("grad_activity", C.c_void_p),
+        ("grad_density_scale", C.c_void_p),
+        ("event_buffer", C.c_void_p),
+        ("event_capacity", C.c_longlong),
+        ("loglik", C.c_double),
+        ("events", C.c_ulonglong),
+        ("replayed", C.c_ulonglong),
+        ("mismatches", C.c_ulonglong),
+        ("forward_ms", C.c_double),
+        ("gradient_ms", C.c_double),
+    ]
+
+
+EVENT_RECORD_BYTES = 24
+
 P = C.c_void_p
 _SIGNATURES = {
     "mcpet_config_read": (C.c_int, [C.c_char_p, C.POINTER(Config)]),
@@ -164,6 +183,7 @@ _SIGNATURES = {
     "mcpet_run": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_device": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_batch": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
+    "mcpet_grad": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies), C.POINTER(GradArgs)]),
     "mcpet_run_batch_device": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_device_noalloc": (C.c_int, [P, P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_last_run_guard": (C.c_int, [P, C.POINTER(C.c_ulonglong)]),

@@ -196,3 +196,28 @@ def test_run_without_gpu_reports_cuda_error(workdir):
     sc = scenes.sample_scene(workdir)
     _expect("cuda", sc.run)
     sc.close()
+
+
+def test_grad_argument_checks(workdir):
+    """mcpet_grad rejects missing inputs before any device work."""
+    import ctypes as C
+    L = _abi.lib()
+    sc = scenes.sample_scene(workdir)
+    t = _abi.Tallies()
+    g = _abi.GradArgs()
+    assert L.mcpet_grad(None, None, C.byref(t), C.byref(g)) == ERR["arg"]
+    assert L.mcpet_grad(sc.handle, None, C.byref(t), C.byref(g)) == ERR["arg"]      # no measured sinogram
+    assert b"measured" in L.mcpet_last_error()
+    g.measured = 16
+    assert L.mcpet_grad(sc.handle, None, C.byref(t), C.byref(g)) == ERR["arg"]      # no forward sinograms
+    assert b"trues and scatter" in L.mcpet_last_error()
+    t.trues, t.scatter = 16, 16
+    g.event_buffer, g.event_capacity = 16, 0
+    assert L.mcpet_grad(sc.handle, None, C.byref(t), C.byref(g)) == ERR["arg"]
+    assert b"event_capacity" in L.mcpet_last_error()
+    sc.close()
+    psf_only = scenes.sample_scene(workdir, tally_psf_sinogram=1)
+    g.event_buffer, g.event_capacity = None, 0
+    assert L.mcpet_grad(psf_only.handle, None, C.byref(t), C.byref(g)) == ERR["arg"]
+    assert b"sinogram tally" in L.mcpet_last_error()
+    psf_only.close()
