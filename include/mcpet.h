@@ -238,6 +238,23 @@ mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
 mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                              mcpet_tallies* outs);
 
+/* PSF records streamed in bounded chunks instead of one buffer of
+ * psf_size * 44 bytes (the reference allocates the whole PSF up front,
+ * MCGPU-PET.cu:2094, and writes it at the end, report_PSF
+ * MCGPU-PET.cu:3193-3322).  The transport runs as consecutive launches over
+ * ranges of lanes -- each lane keeps its RANECU stream, so the set of
+ * records and the tallies equal one mcpet_run with an unbounded PSF --
+ * and after each launch the sink receives that launch's packed 44-byte
+ * records (at most chunk_records of them; order within and across chunks
+ * is not specified, as in the reference).  A range whose records overflow
+ * the chunk is replayed in halves with its sinogram-side writes suppressed.
+ * Returning nonzero from the sink stops the run.  out receives the
+ * sinograms/images/spectrum/totals as in mcpet_run (out->psf is ignored;
+ * *out->psf_count = records streamed).  Blocking. */
+typedef int (*mcpet_psf_sink)(const void* records, long long n_records, void* user);
+mcpet_status mcpet_run_psf_stream(mcpet_scene* scene, const mcpet_run_opts* opts, long long chunk_records,
+                                  mcpet_psf_sink sink, void* user, mcpet_tallies* out);
+
 /* Gradient of the Poisson log-likelihood of a measured sinogram,
  *   L = sum_b y_b ln(lambda_b) - lambda_b,  lambda = trues + scatter + background,
  * with respect to each voxel's activity and density scale.  No counterpart

@@ -355,6 +355,9 @@ int pick_block(const mcpet_run_opts& o) {
   return block < 32 ? 32 : block;
 }
 
+mcpet_status launch_planned(mcpet_scene* sc, const mcpet_run_opts& o, TransportParams& P, DeviceTallies& O,
+                            cudaStream_t st, double* ms_out);
+
 /* Enqueue one transport run writing into the device tallies O. */
 mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTallies O, cudaStream_t st,
                          double* ms_out) {
@@ -386,6 +389,14 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   CUDA_TRY(cudaMemsetAsync(small, 0, 2 * sizeof(unsigned long long), st));
   if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
 
+  return launch_planned(sc, o, P, O, st, ms_out);
+}
+
+/* Launch the transport for a prepared run (P, O complete, the work-queue
+ * word set), optionally timed. */
+mcpet_status launch_planned(mcpet_scene* sc, const mcpet_run_opts& o, TransportParams& P, DeviceTallies& O,
+                            cudaStream_t st, double* ms_out) {
+  auto& d = sc->dev;
   const bool counters = o.collect_counters && O.counters;
   const int block = pick_block(o);
   int algorithm = o.algorithm == kAlgorithmHistories ? kAlgorithmHistories : kAlgorithmEvents;
@@ -1074,6 +1085,141 @@ mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_talli
   g->forward_ms = fwd_ms;
   g->gradient_ms = gms;
   return MCPET_OK;
+}
+
+mcpet_status mcpet_run_psf_stream(mcpet_scene* sc, const mcpet_run_opts* opts, long long chunk_records,
+                                  mcpet_psf_sink sink, void* user, mcpet_tallies* out) {
+  if (!sc || !sink || !out) return set_error(MCPET_ERR_ARG, "null argument");
+  if (!(sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 1))
+    return set_error(MCPET_ERR_ARG, "the scene does not tally a PSF (REPORT PSF/SINOGRAM 0 or 1)");
+  if (chunk_records < 2 || chunk_records > 0x7fffffffLL)
+    return set_error(MCPET_ERR_ARG, "chunk_records must be in [2, 2^31)");
+  mcpet_status s = validate_opts(sc, opts);
+  if (s != MCPET_OK) return s;
+  s = ensure_device(sc);
+  if (s != MCPET_OK) return s;
+  s = upload_tables(sc);
+  if (s != MCPET_OK) return s;
+  s = ensure_run_buffers(sc, false);
+  if (s != MCPET_OK) return s;
+  mcpet_run_opts def;
+  memset(&def, 0, sizeof(def));
+  const mcpet_run_opts& o = opts ? *opts : def;
+  const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
+  const int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
+  sc->dev.run_h2d = 0;
+  s = build_lanes(sc, o.lane_mode, tpb, hpl);
+  if (s != MCPET_OK) return s;
+  auto& d = sc->dev;
+  cudaStream_t st = (cudaStream_t)o.stream;
+
+  DeviceTallies O;
+  memset(&O, 0, sizeof(O));
+  O.trues = d.trues;
+  O.scatter = d.scatter;
+  O.image_trues = d.img_t;
+  O.image_scatter = d.img_s;
+  O.spectrum = d.spectrum;
+  O.histories = d.small + 2;
+  O.psf_count = (int*)(d.small + 3);
+  O.coincidences = d.small + 14;
+  O.counters = o.collect_counters ? d.small + 4 : nullptr;
+  TransportParams P;
+  s = prepare_run(sc, o, O, st, P);
+  if (s != MCPET_OK) return s;
+  O.guard = d.small + 0;
+  O.lane_cursor = d.small + 1;
+  CUDA_TRY(cudaMemsetAsync(d.small, 0, 2 * sizeof(unsigned long long), st));
+  if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
+  if (!d.gwords) CUDA_TRY(dmalloc(&d.gwords, 4 * sizeof(unsigned long long)));
+
+  uint32_t* chunk = nullptr;
+  CUDA_TRY(dmalloc(&chunk, (size_t)chunk_records * 44));
+  std::vector<unsigned char> host((size_t)chunk_records * 44);
+  O.psf = chunk;
+  P.psf_capacity = (int)chunk_records;
+  P.n_emitters = d.n_emitters;
+  const uint64_t total = d.n_lanes;
+  long long streamed = 0;
+  double ms_sum = 0;
+  mcpet_status err = MCPET_OK;
+
+  /* one launch over lanes [b, e): dry = replay of a range whose records did
+   * not fit (no sinogram-side writes, totals to scratch words) */
+  auto run_range = [&](uint64_t b, uint64_t e, bool dry, int& count) -> mcpet_status {
+    TransportParams Q = P;
+    DeviceTallies R = O;
+    Q.n_lanes = e;
+    Q.sino_dry = dry ? 1 : 0;
+    if (dry) {
+      R.histories = d.gwords + 0;
+      R.coincidences = d.gwords + 1;
+      R.counters = nullptr;
+    }
+    unsigned long long begin = b;
+    CUDA_TRY(cudaMemcpyAsync(O.lane_cursor, &begin, sizeof(begin), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(O.psf_count, 0, 4, st));
+    double ms = 0;
+    mcpet_status r = launch_planned(sc, o, Q, R, st, &ms);
+    if (r != MCPET_OK) return r;
+    ms_sum += ms;
+    CUDA_TRY(cudaMemcpyAsync(&count, O.psf_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return MCPET_OK;
+  };
+  auto drain = [&](int count) -> mcpet_status {
+    if (count <= 0) return MCPET_OK;
+    CUDA_TRY(cudaMemcpy(host.data(), chunk, (size_t)count * 44, cudaMemcpyDeviceToHost));
+    streamed += count;
+    if (sink(host.data(), count, user) != 0) return set_error(MCPET_ERR_ARG, "the PSF sink stopped the run");
+    return MCPET_OK;
+  };
+  /* ranges whose records overflowed the chunk, replayed in halves */
+  std::vector<std::pair<uint64_t, uint64_t>> redo;
+  uint64_t b = 0, span = std::max<uint64_t>(1, total / 64);
+  while (err == MCPET_OK && b < total) {
+    const uint64_t e = std::min<uint64_t>(total, b + span);
+    int count = 0;
+    err = run_range(b, e, false, count);
+    if (err != MCPET_OK) break;
+    if (count <= chunk_records) {
+      err = drain(count);
+      const double per_lane = (double)std::max(count, 1) / (double)(e - b);
+      span = std::max<uint64_t>(1, (uint64_t)(0.5 * (double)chunk_records / per_lane));
+    } else {
+      redo.push_back({b, e});
+      span = std::max<uint64_t>(1, (e - b) / 4);
+    }
+    b = e;
+  }
+  while (err == MCPET_OK && !redo.empty()) {
+    auto r = redo.back();
+    redo.pop_back();
+    int count = 0;
+    err = run_range(r.first, r.second, true, count);
+    if (err != MCPET_OK) break;
+    if (count <= chunk_records) {
+      err = drain(count);
+    } else if (r.second - r.first == 1) {
+      err = set_error(MCPET_ERR_LIMIT, "one lane produced %d PSF records, more than a chunk of %lld", count,
+                      chunk_records);
+    } else {
+      const uint64_t m = r.first + (r.second - r.first) / 2;
+      redo.push_back({m, r.second});
+      redo.push_back({r.first, m});
+    }
+  }
+  dfree(chunk);
+  if (err != MCPET_OK) return err;
+  /* sinograms, images, spectrum and totals as mcpet_run reports them */
+  mcpet_tallies t = *out;
+  t.psf = nullptr;
+  t.psf_capacity = 0;
+  int dummy = 0;
+  t.psf_count = &dummy;
+  s = download_run(sc, opts, &t, false, ms_sum, st);
+  if (out->psf_count) *out->psf_count = (int)std::min<long long>(streamed, 0x7fffffff);
+  return s;
 }
 
 mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_device, const mcpet_run_opts* opts,

@@ -221,17 +221,18 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
           float ea = a.energy + (P.e_resol / 2.35f) * a.energy * g2;
           int ib = __float2int_rd(eb / 1000.0f);
           int ia = __float2int_rd(ea / 1000.0f);
-          if ((ib < P.ne) && (ib >= 0)) {
+          /* sino_dry: the same draws, no sinogram-side writes (a PSF replay) */
+          if ((ib < P.ne) && (ib >= 0) && !P.sino_dry) {
             if (spec_sh) atomicAdd(&spec_sh[ib], 1);
             else atomicAdd(&O.spectrum[ib], 1);
             Counting<kCount>::add(cnt.tallies, 1);
           }
-          if ((ia < P.ne) && (ia >= 0)) {
+          if ((ia < P.ne) && (ia >= 0) && !P.sino_dry) {
             if (spec_sh) atomicAdd(&spec_sh[ia], 1);
             else atomicAdd(&O.spectrum[ia], 1);
             Counting<kCount>::add(cnt.tallies, 1);
           }
-          if (eb > P.e_low && eb < P.e_high && ea > P.e_low && ea < P.e_high) {
+          if (eb > P.e_low && eb < P.e_high && ea > P.e_low && ea < P.e_high && !P.sino_dry) {
             if (bin < P.nbins) {
               if (b.state == 0 && a.state == 0) {
                 atomicAdd(&O.trues[bin], 1);

@@ -94,6 +94,7 @@ struct TransportParams {
   int quorum_scatter;     /* event loop: lanes needed to run a scattering round */
   int quorum_pair;        /* ... and a pair-bookkeeping (end of photon, next decay) round */
   int step_keep;          /* Woodcock batches continue while step_keep/8 of the stepping lanes step */
+  int sino_dry;           /* 1: detector draws as usual but no sinogram, image, spectrum writes */
 };
 
 /* Device pointers of one scene (all read-only during transport). */

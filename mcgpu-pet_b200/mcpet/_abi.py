@@ -169,6 +169,8 @@ class GradArgs(C.Structure):
 
 EVENT_RECORD_BYTES = 24
 
+PSF_SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_longlong, C.c_void_p)
+
 P = C.c_void_p
 _SIGNATURES = {
     "mcpet_config_read": (C.c_int, [C.c_char_p, C.POINTER(Config)]),
@@ -184,6 +186,7 @@ _SIGNATURES = {
     "mcpet_run_device": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_batch": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_grad": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies), C.POINTER(GradArgs)]),
+    "mcpet_run_psf_stream": (C.c_int, [P, C.POINTER(RunOpts), C.c_longlong, P, P, C.POINTER(Tallies)]),
     "mcpet_run_batch_device": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_device_noalloc": (C.c_int, [P, P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_last_run_guard": (C.c_int, [P, C.POINTER(C.c_ulonglong)]),

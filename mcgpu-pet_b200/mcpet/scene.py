@@ -246,6 +246,34 @@ class Scene:
         check(lib().mcpet_run(self._h, C.byref(co), C.byref(h.t)))
         return h.result()
 
+    def run_psf_stream(self, chunk_records: int, opts: Optional[RunOptions] = None, sink=None) -> RunResult:
+        """Run with the PSF streamed in chunks (mcpet_run_psf_stream).  sink(records)
+        receives each chunk as a PSF_DTYPE array; without a sink the chunks
+        are concatenated into RunResult.psf."""
+        opts = opts or RunOptions()
+        h = self._host_run(0)
+        chunks = []
+
+        def _cb(ptr, n, _user):
+            try:
+                buf = (C.c_ubyte * (int(n) * _abi.PSF_RECORD_BYTES)).from_address(ptr)
+                rec = np.frombuffer(bytes(buf), dtype=PSF_DTYPE)
+                if sink is not None:
+                    return 1 if sink(rec) is False else 0
+                chunks.append(rec)
+                return 0
+            except Exception:       # never let an exception cross the C boundary
+                return 1
+
+        cb = _abi.PSF_SINK(_cb)
+        co = opts.to_c()
+        check(lib().mcpet_run_psf_stream(self._h, C.byref(co), int(chunk_records), C.cast(cb, C.c_void_p), None,
+                                         C.byref(h.t)))
+        r = h.result()
+        r.psf = np.concatenate(chunks) if chunks else np.zeros(0, PSF_DTYPE)
+        r.psf_count = int(h.psf_count.value)
+        return r
+
     @staticmethod
     def run_batch(scenes: list, opts: Optional[RunOptions] = None,
                   psf_capacity: Optional[int] = None) -> list:

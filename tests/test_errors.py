@@ -221,3 +221,19 @@ def test_grad_argument_checks(workdir):
     assert L.mcpet_grad(psf_only.handle, None, C.byref(t), C.byref(g)) == ERR["arg"]
     assert b"sinogram tally" in L.mcpet_last_error()
     psf_only.close()
+
+
+def test_psf_stream_argument_checks(workdir):
+    import ctypes as C
+    L = _abi.lib()
+    t = _abi.Tallies()
+    sino_only = scenes.sample_scene(workdir, tally_psf_sinogram=2)
+    cb = _abi.PSF_SINK(lambda p, n, u: 0)
+    assert L.mcpet_run_psf_stream(sino_only.handle, None, 64, C.cast(cb, C.c_void_p), None, C.byref(t)) == ERR["arg"]
+    assert b"does not tally a PSF" in L.mcpet_last_error()
+    sino_only.close()
+    psf = scenes.sample_scene(workdir, tally_psf_sinogram=1)
+    assert L.mcpet_run_psf_stream(psf.handle, None, 1, C.cast(cb, C.c_void_p), None, C.byref(t)) == ERR["arg"]
+    assert b"chunk_records" in L.mcpet_last_error()
+    assert L.mcpet_run_psf_stream(psf.handle, None, 64, None, None, C.byref(t)) == ERR["arg"]
+    psf.close()
