@@ -115,6 +115,7 @@ typedef struct {
   int n_emitters;                 /* lane plan of the last run */
   long long n_lanes;
   long long last_h2d_bytes;       /* bytes copied host->device by the last run */
+  long long n_dose_voxels;        /* voxels of the dose ROI (0 when the voxel dose tally is off) */
 } mcpet_scene_info;
 
 typedef struct {
@@ -157,6 +158,12 @@ typedef struct {
   unsigned long long* coincidences;     /* detected pairs = sum(trues) + sum(scatter) */
   mcpet_counters* counters;
   double* transport_ms;           /* device time of the transport kernel(s) */
+  /* dose tallies (when the input enables them; tally_materials_dose and
+   * tally_voxel_energy_deposition, MCGPU-PET_kernel.cu:396-410, 1593-1650):
+   * per pair {sum of Edep in eV (SCALE_eV = 1), sum of Edep^2}, each term
+   * rounded to an integer as the reference's device build does */
+  unsigned long long* material_dose;    /* [MCPET_MAX_MATERIALS][2] or NULL */
+  unsigned long long* voxel_dose;       /* [n_dose_voxels][2] ROI voxels, x fastest, or NULL */
 } mcpet_tallies;
 
 /* ---- configuration and scene (host) ---------------------------------- */
@@ -266,7 +273,8 @@ mcpet_status mcpet_run_psf_stream(mcpet_scene* scene, const mcpet_run_opts* opts
  * tallied history is recomputed from the RANECU state recorded at its
  * emission and each Woodcock step inside a voxel adds w_b times
  * d ln p(step)/d ln rho to it.  A replay that does not reproduce the recorded
- * bin is left out of dL/ds and counted in mismatches.  Blocking. */
+ * bin is left out of dL/ds and counted in mismatches.  The forward of this
+ * call does not produce the dose tallies.  Blocking. */
 typedef struct {
   const float* measured;          /* device [n_bins]: y, the measured sinogram (counts) */
   const float* background;        /* device [n_bins]: r, expected background added to the model; NULL = 0 */

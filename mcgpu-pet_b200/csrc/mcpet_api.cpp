@@ -131,6 +131,7 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.spectrum_in_shared = (c.n_energy_bins > 0 && c.n_energy_bins <= kSpectrumSharedMax) ? 1 : 0;
   P.palette_in_shared = (sc->palette.size() <= 2048) ? (int)sc->palette.size() : 0;
   P.e_annihilation = 510998.95f;
+  for (int k = 0; k < 6; ++k) P.dose_roi[k] = c.tally_voxel_dose ? c.dose_roi[k] : (k % 2 ? -1 : 0);
   P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 16, 1, 32);
   P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 32, 1, 32);
   P.step_keep = env_int("MCPET_STEP_KEEP", 2, 1, 8);
@@ -343,6 +344,10 @@ mcpet_status prepare_run(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies
   CUDA_TRY(cudaMemsetAsync(O.histories, 0, 8, st));
   if (!O.coincidences) O.coincidences = sc->dev.small + 14;
   CUDA_TRY(cudaMemsetAsync(O.coincidences, 0, 8, st));
+  if (!sc->cfg.tally_material_dose) O.mat_dose = nullptr;
+  if (dose_voxels(sc->cfg) == 0) O.vox_dose = nullptr;
+  if (O.mat_dose) CUDA_TRY(cudaMemsetAsync(O.mat_dose, 0, 2 * kMaxMaterials * 8, st));
+  if (O.vox_dose) CUDA_TRY(cudaMemsetAsync(O.vox_dose, 0, (size_t)dose_voxels(sc->cfg) * 16, st));
   /* the kernel only touches the spectrum when the sinogram is tallied */
   if (!sino) P.spectrum_in_shared = 0;
   return MCPET_OK;
@@ -402,6 +407,7 @@ mcpet_status launch_planned(mcpet_scene* sc, const mcpet_run_opts& o, TransportP
   int algorithm = o.algorithm == kAlgorithmHistories ? kAlgorithmHistories : kAlgorithmEvents;
   if (algorithm == kAlgorithmEvents && env_int("MCPET_MINBLOCKS", 4, 1, 4) == 1) algorithm = kAlgorithmEventsUncapped;
   if (O.events && algorithm != kAlgorithmHistories) algorithm = kAlgorithmEventsRecord;
+  else if ((O.mat_dose || O.vox_dose) && algorithm != kAlgorithmHistories) algorithm = kAlgorithmEventsDose;
   size_t smem = transport_dynamic_smem(P, block, algorithm);
   int bps = 0;
   CUDA_TRY(transport_occupancy(counters, algorithm, block, smem, &bps));
@@ -445,6 +451,13 @@ mcpet_status ensure_run_buffers(mcpet_scene* sc, bool want_psf) {
     CUDA_TRY(dmalloc(&d.spectrum, (size_t)std::max(ne, 1) * 4));
     d.ne_alloc = ne;
   }
+  if (sc->cfg.tally_material_dose && !d.mdose) CUDA_TRY(dmalloc(&d.mdose, 2 * kMaxMaterials * 8));
+  const long long nd = dose_voxels(sc->cfg);
+  if (nd != d.vdose_alloc) {
+    dfree(d.vdose);
+    if (nd > 0) CUDA_TRY(dmalloc(&d.vdose, (size_t)nd * 16));
+    d.vdose_alloc = nd;
+  }
   long long cap = want_psf ? (long long)std::max(sc->cfg.psf_size, 0) : 0;
   if (cap != d.psf_cap) {
     dfree(d.psf);
@@ -475,6 +488,8 @@ mcpet_scene::~mcpet_scene() {
     dfree(dev.psf);
     dfree(dev.small);
     dfree(dev.events);
+    dfree(dev.mdose);
+    dfree(dev.vdose);
     dfree(dev.activity);
     dfree(dev.gwords);
     if (dev.ev0) cudaEventDestroy((cudaEvent_t)dev.ev0);
@@ -494,6 +509,11 @@ mcpet_status download_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tal
   if (out->image_scatter) CUDA_TRY(cudaMemcpyAsync(out->image_scatter, d.img_s, nv, cudaMemcpyDeviceToHost, st));
   if (out->spectrum)
     CUDA_TRY(cudaMemcpyAsync(out->spectrum, d.spectrum, (size_t)sc->cfg.n_energy_bins * 4, cudaMemcpyDeviceToHost,
+                             st));
+  if (out->material_dose && d.mdose && sc->cfg.tally_material_dose)
+    CUDA_TRY(cudaMemcpyAsync(out->material_dose, d.mdose, 2 * kMaxMaterials * 8, cudaMemcpyDeviceToHost, st));
+  if (out->voxel_dose && d.vdose && dose_voxels(sc->cfg) > 0)
+    CUDA_TRY(cudaMemcpyAsync(out->voxel_dose, d.vdose, (size_t)dose_voxels(sc->cfg) * 16, cudaMemcpyDeviceToHost,
                              st));
   unsigned long long small[16];
   CUDA_TRY(cudaMemcpyAsync(small, d.small, sizeof(small), cudaMemcpyDeviceToHost, st));
@@ -692,14 +712,16 @@ mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_op
   const int block = pick_block(o);
   const size_t smem = transport_dynamic_smem(P, block, kAlgorithmEvents);
   int bps = 0;
-  CUDA_TRY(transport_batch_occupancy(counters, block, smem, &bps));
+  bool dose = false;
+  for (const SceneSlot& z : slots) dose = dose || z.O.mat_dose || z.O.vox_dose;
+  CUDA_TRY(transport_batch_occupancy(counters, dose, block, smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   const int grid = total == 0 ? 1 : s0->dev.sm_count * bps;
   auto& d = s0->dev;
   if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
-  CUDA_TRY(launch_transport_batch(P, T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, counters, grid, block, smem,
-                                  st));
+  CUDA_TRY(launch_transport_batch(P, T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, counters, dose, grid, block,
+                                  smem, st));
   if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
   CUDA_TRY(cudaFreeAsync(dbuf, st));
   if (ms_out) {
@@ -724,6 +746,8 @@ DeviceTallies tallies_from(const mcpet_tallies* out) {
   O.histories = out->total_histories;
   O.coincidences = out->coincidences;
   O.counters = (unsigned long long*)out->counters;
+  O.mat_dose = out->material_dose;
+  O.vox_dose = out->voxel_dose;
   return O;
 }
 
@@ -829,6 +853,7 @@ mcpet_status mcpet_scene_get_info(const mcpet_scene* sc, mcpet_scene_info* info)
   info->n_emitters = sc->dev.n_emitters;
   info->n_lanes = (long long)sc->dev.n_lanes;
   info->last_h2d_bytes = sc->dev.last_h2d;
+  info->n_dose_voxels = dose_voxels(sc->cfg);
   return MCPET_OK;
 }
 
@@ -890,6 +915,8 @@ mcpet_status mcpet_run_device(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet
   O.histories = out->total_histories;
   O.coincidences = out->coincidences;
   O.counters = (unsigned long long*)out->counters;
+  O.mat_dose = out->material_dose;
+  O.vox_dose = out->voxel_dose;
   cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
   double ms = 0;
   mcpet_status s = enqueue_run(sc, opts, O, st, out->transport_ms ? &ms : nullptr);
@@ -921,6 +948,8 @@ mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallie
   O.psf_count = (int*)(d.small + 3);
   O.coincidences = d.small + 14;
   O.counters = (opts && opts->collect_counters) ? d.small + 4 : nullptr;
+  O.mat_dose = out->material_dose ? d.mdose : nullptr;
+  O.vox_dose = out->voxel_dose ? d.vdose : nullptr;
   cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
   double ms = 0;
   s = enqueue_run(sc, opts, O, st, &ms);
@@ -972,6 +1001,8 @@ mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcp
     z.psf_count = (int*)(d.small + 3);
     z.coincidences = d.small + 14;
     z.counters = (k == 0 && opts && opts->collect_counters) ? d.small + 4 : nullptr;
+    z.mat_dose = outs[k].material_dose ? d.mdose : nullptr;
+    z.vox_dose = outs[k].voxel_dose ? d.vdose : nullptr;
   }
   cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
   double ms = 0;
@@ -1032,6 +1063,8 @@ mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_talli
       cap = d.event_cap;
     }
     DeviceTallies O = tallies_from(device_out);
+    O.mat_dose = nullptr;   /* the recording forward does not tally dose */
+    O.vox_dose = nullptr;
     O.events = ev;
     O.event_count = d.small + 15;
     O.event_capacity = cap;
@@ -1124,6 +1157,8 @@ mcpet_status mcpet_run_psf_stream(mcpet_scene* sc, const mcpet_run_opts* opts, l
   O.psf_count = (int*)(d.small + 3);
   O.coincidences = d.small + 14;
   O.counters = o.collect_counters ? d.small + 4 : nullptr;
+  O.mat_dose = out->material_dose ? d.mdose : nullptr;
+  O.vox_dose = out->voxel_dose ? d.vdose : nullptr;
   TransportParams P;
   s = prepare_run(sc, o, O, st, P);
   if (s != MCPET_OK) return s;
@@ -1155,6 +1190,8 @@ mcpet_status mcpet_run_psf_stream(mcpet_scene* sc, const mcpet_run_opts* opts, l
       R.histories = d.gwords + 0;
       R.coincidences = d.gwords + 1;
       R.counters = nullptr;
+      R.mat_dose = nullptr;
+      R.vox_dose = nullptr;
     }
     unsigned long long begin = b;
     CUDA_TRY(cudaMemcpyAsync(O.lane_cursor, &begin, sizeof(begin), cudaMemcpyHostToDevice, st));

@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <sys/time.h>
 #include <zlib.h>
 
@@ -538,9 +539,25 @@ mcpet_status load_materials(mcpet_scene* sc) {
   return MCPET_OK;
 }
 
+/* Voxels of the dose ROI (0 when the voxel dose tally is off). */
+long long dose_voxels(const mcpet_config& c) {
+  const short* r = c.dose_roi;
+  if (!c.tally_voxel_dose || r[1] < 0) return 0;
+  return (long long)(r[1] - r[0] + 1) * (long long)(r[3] - r[2] + 1) * (long long)(r[5] - r[4] + 1);
+}
+
 /* Checks after loading (MCGPU-PET.cu:316-351) and palette compression. */
 mcpet_status finalize_scene(mcpet_scene* sc) {
   mcpet_config& cfg = sc->cfg;
+  if (cfg.tally_voxel_dose) {
+    /* the ROI's upper corner is clipped to the phantom (load_voxels, MCGPU-PET.cu:1444-1452) */
+    short* r = cfg.dose_roi;
+    r[1] = (short)std::min<int>(sc->nx - 1, r[1]);
+    r[3] = (short)std::min<int>(sc->ny - 1, r[3]);
+    r[5] = (short)std::min<int>(sc->nz - 1, r[5]);
+    if (r[0] > r[1] || r[2] > r[3] || r[4] > r[5])
+      return set_error(MCPET_ERR_FORMAT, "the dose region of interest lies outside the phantom");
+  }
   for (long long i = 0; i < (long long)sc->mat0.size(); ++i)
     if (!sc->material_loaded[sc->mat0[i]])
       return set_error(MCPET_ERR_FORMAT, "voxel %lld uses material %d which has no material file", i + 1,
@@ -608,6 +625,113 @@ struct PsfView {
   int n(long long i, int off) const { int v; memcpy(&v, base + 44 * i + off, 4); return v; }
   short s(long long i, int off) const { short v; memcpy(&v, base + 44 * i + off, 2); return v; }
 };
+
+/* Materials dose report (report_materials_dose, MCGPU-PET.cu:2664-2725): per
+ * defined material, dose = sum(Edep)/N/mass with mass = sum over the
+ * phantom's voxels of density x voxel volume, and its 2-sigma uncertainty
+ * from sum(Edep^2). */
+std::string format_materials_dose(const mcpet_scene* sc, const unsigned long long* md, unsigned long long n_hist) {
+  const double vol = 1.0 / ((double)sc->inv_voxel_size[0] * (double)sc->inv_voxel_size[1] *
+                            (double)sc->inv_voxel_size[2]);
+  double mass[kMaxMaterials] = {0};
+  for (size_t v = 0; v < sc->mat0.size(); ++v) mass[sc->mat0[v]] += (double)sc->rho[v] * vol;
+  const double inv_n = 1.0 / (double)(n_hist ? n_hist : 1);
+  std::string out;
+  char line[1024];
+  snprintf(line, sizeof(line), "\n          *** MATERIALS TOTAL DOSE TALLY REPORT ***\n\n"
+           "              Total number of simulated x rays: %llu\n\n"
+           "\t [MAT]  [DOSE eV/g/hist]  [2*std_dev]  [Rel_error 2*std_dev, %%]  [E_dep eV/hist]  [DOSE mGy]  "
+           "[Material mass g]  [Material file name]\n", n_hist);
+  out += line;
+  for (int m = 0; m < kMaxMaterials; ++m) {
+    if (sc->density_nominal[m] < 0.0f) break;
+    const char* name = sc->cfg.material_files[m];
+    const char* slash = strrchr(name, '/');
+    if (slash) name = slash + 1;
+    const double edep = (double)md[2 * m] * inv_n;
+    double sd = sqrt(((double)md[2 * m + 1] * inv_n - edep * edep) * inv_n);
+    const double rel = edep > 0.0 ? sd / edep : 0.0;
+    const double m_g = std::max(mass[m], 0.00001);
+    snprintf(line, sizeof(line), "\t%d\t%.5lf\t\t%.5lf\t\t%.2lf\t\t%.5lf\t\t%.5lf\t\t%.5lf\t\t%s\n", m + 1, edep / m_g,
+             2.0 * sd / m_g, 200.0 * rel, edep, (double)md[2 * m] / m_g * (1.0e3 / 6.2415e15), mass[m], name);
+    out += line;
+  }
+  return out;
+}
+
+/* Voxel dose in the ROI (report_voxels_dose, MCGPU-PET.cu:2389-2640): the
+ * text file holds the central Z plane of the ROI (dose and 2 sigma, eV/g per
+ * history; one blank line between Y rows), the .raw files the whole ROI as
+ * 32-bit floats (dose; % relative error at 2 sigma), x fastest.  Voxels of
+ * density below 0.1 g/cm^3 (air) report 0. */
+static mcpet_status write_voxel_dose(const mcpet_scene* sc, const mcpet_tallies* t, const std::string& path,
+                                     double elapsed_s) {
+  const mcpet_config& c = sc->cfg;
+  const short* r = c.dose_roi;
+  const int dx = r[1] - r[0] + 1, dy = r[3] - r[2] + 1, dz = r[5] - r[4] + 1;
+  const int zplane = (r[5] + r[4]) / 2 - r[4];
+  const unsigned long long n_hist = t->total_histories ? *t->total_histories : 0ull;
+  const double inv_n = 1.0 / (double)(n_hist ? n_hist : 1);
+  const double vol = 1.0 / ((double)sc->inv_voxel_size[0] * (double)sc->inv_voxel_size[1] *
+                            (double)sc->inv_voxel_size[2]);
+  FILE* f = fopen(path.c_str(), "w");
+  if (!f) return set_error(MCPET_ERR_IO, "cannot write '%s'", path.c_str());
+  const std::string pm = path + ".raw", ps = path + "_PercentRelError2sigma.raw";
+  FILE* fm = fopen(pm.c_str(), "wb");
+  FILE* fs = fopen(ps.c_str(), "wb");
+  if (!fm || !fs) {
+    fclose(f);
+    if (fm) fclose(fm);
+    if (fs) fclose(fs);
+    return set_error(MCPET_ERR_IO, "cannot write '%s'", pm.c_str());
+  }
+  fprintf(f, "#\n#  3D voxel dose (photon KERMA: energy deposited by photon interactions in each voxel, no electron\n"
+             "#  transport) in the region of interest; 32-bit float binaries: %s (dose) and %s (%% relative error\n"
+             "#  at 2 standard deviations).  This text: the ROI plane z_coord = %d (z_coord in ROI = %d).\n#\n",
+          pm.c_str(), ps.c_str(), zplane + r[4], zplane);
+  fprintf(f, "#  Voxel size:  %lf x %lf x %lf = %lf cm^3\n", 1.0 / (double)sc->inv_voxel_size[0],
+          1.0 / (double)sc->inv_voxel_size[1], 1.0 / (double)sc->inv_voxel_size[2], vol);
+  fprintf(f, "#  Number of voxels in the reported region of interest (ROI) X, Y and Z:\n#      %d  %d  %d\n", dx, dy,
+          dz);
+  fprintf(f, "#  Coordinates of the ROI inside the voxel volume = X[%d,%d], Y[%d,%d], Z[%d,%d]\n", r[0] + 1, r[1] + 1,
+          r[2] + 1, r[3] + 1, r[4] + 1, r[5] + 1);
+  fprintf(f, "#  Voxel dose units: eV/g per history\n#\n#    [DOSE]   [2*standard_deviation]\n"
+             "# =====================================\n");
+  unsigned long long total = 0;
+  long long k = 0;
+  for (int z = 0; z < dz; ++z) {
+    for (int y = 0; y < dy; ++y) {
+      for (int x = 0; x < dx; ++x, ++k) {
+        const size_t g = (size_t)(x + r[0]) + (size_t)(y + r[2]) * sc->nx + (size_t)(z + r[4]) * sc->nx * sc->ny;
+        const double rho = sc->rho[g];
+        unsigned long long e1 = t->voxel_dose[2 * k], e2 = t->voxel_dose[2 * k + 1];
+        if (rho < 0.1) e1 = e2 = 0;
+        const double inv_mass = 1.0 / (rho * vol);
+        double dose = (double)e1 * inv_n;
+        total += e1;
+        double sd = ((double)e2 * inv_n - dose * dose) * inv_n * inv_mass;
+        if (sd > 0.0) sd = sqrt(sd);
+        dose *= inv_mass;
+        if (z == zplane) fprintf(f, "%.6lf %.6lf\n", dose, 2.0 * sd);
+        const float df = (float)dose;
+        const float ef = dose > 0.0 ? 200.0f * (float)(sd / dose) : 0.0f;
+        fwrite(&df, sizeof(float), 1, fm);
+        fwrite(&ef, sizeof(float), 1, fs);
+      }
+      if (z == zplane) fprintf(f, "\n");
+    }
+    if (z == zplane) fprintf(f, "\n");
+  }
+  fprintf(f, "#   ****** DOSE REPORT: TOTAL SIMULATION PERFORMANCE ******\n");
+  fprintf(f, "#       Total number of simulated x rays: %llu\n", n_hist);
+  fprintf(f, "#       Total simulation time [s]:  %.2f\n", elapsed_s);
+  fprintf(f, "\n#       Total energy absorved inside the dose ROI: %.5lf keV/hist\n\n",
+          0.001 * (double)total * inv_n);
+  fclose(f);
+  fclose(fm);
+  fclose(fs);
+  return MCPET_OK;
+}
 
 mcpet_status write_outputs(const mcpet_scene* sc, const mcpet_tallies* t, const char* out_dir, int bg,
                            double elapsed_s) {
@@ -683,6 +807,18 @@ mcpet_status write_outputs(const mcpet_scene* sc, const mcpet_tallies* t, const 
     if (elapsed_s > 0.000001) fprintf(f, "#       Speed [x-rays/s]:    %.2f\n\n", ((double)hist) / elapsed_s);
     fclose(f);
     fclose(fb);
+  }
+  if (c.tally_voxel_dose && t->voxel_dose && dose_voxels(c) > 0) {
+    mcpet_status s = write_voxel_dose(sc, t, join(out_dir, c.dose_file), elapsed_s);
+    if (s != MCPET_OK) return s;
+  }
+  if (c.tally_material_dose && t->material_dose) {
+    std::string p = join(out_dir, "materials_dose.txt");
+    FILE* f = fopen(p.c_str(), "w");
+    if (!f) return set_error(MCPET_ERR_IO, "cannot write '%s'", p.c_str());
+    const std::string txt = format_materials_dose(sc, t->material_dose, t->total_histories ? *t->total_histories : 0);
+    fputs(txt.c_str(), f);
+    fclose(f);
   }
   return MCPET_OK;
 }

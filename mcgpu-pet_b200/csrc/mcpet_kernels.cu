@@ -74,6 +74,40 @@ struct PhotonState {
   int state;    /* 0 unscattered, 1 Compton, 2 Rayleigh, 3 multiple */
 };
 
+/* Dose of one real interaction (MCGPU-PET_kernel.cu:396-410): `loss` is the
+ * reference's temporary, E_after - E_before for Compton and -E for
+ * photoelectric absorption; energy is deposited when it is below -0.001 eV.
+ * Material sums go to `mat` (a block's shared copy, or global memory), the
+ * ROI voxel sums to global memory, each term rounded to an integer as the
+ * device build of tally_materials_dose / tally_voxel_energy_deposition does
+ * (MCGPU-PET_kernel.cu:1593-1650; SCALE_eV = 1). */
+struct DoseSink {
+  unsigned long long* mat;   /* [15][2] or NULL */
+  unsigned long long* vox;   /* [ROI][2] or NULL */
+  __device__ __forceinline__ void operator()(const TransportParams& P, float loss, int material,
+                                             const float3& pos) const {
+    if (!(loss < -0.001f)) return;
+    const float edep = -1.0f * loss;
+    const unsigned long long e1 = __float2ull_rn(edep), e2 = __float2ull_rn(edep * edep);
+    if (mat) {
+      atomicAdd(&mat[2 * material], e1);
+      atomicAdd(&mat[2 * material + 1], e2);
+    }
+    if (vox) {
+      const int x = __float2int_rd(pos.x * P.inv_vx);
+      const int y = __float2int_rd(pos.y * P.inv_vy);
+      const int z = __float2int_rd(pos.z * P.inv_vz);
+      const int* r = P.dose_roi;
+      if (x < r[0] || x > r[1] || y < r[2] || y > r[3] || z < r[4] || z > r[5]) return;
+      const int dx = 1 + r[1] - r[0];
+      const long long k = (long long)(x - r[0]) + (long long)(y - r[2]) * dx +
+                          (long long)(z - r[4]) * dx * (1 + r[3] - r[2]);
+      atomicAdd(&vox[2 * k], e1);
+      atomicAdd(&vox[2 * k + 1], e2);
+    }
+  }
+};
+
 /* Observer of the Woodcock steps inside the phantom: voxel, whether the
  * step ended in a real interaction, and the probability of a virtual one. */
 struct NoStepHook {
@@ -86,7 +120,8 @@ struct NoStepHook {
 template <bool kCount, typename Scratch, typename Hook = NoStepHook>
 __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P, const DeviceTables& T,
                                              const PaletteEntry* pal, const ComptonTable& C, Scratch rn,
-                                             PhotonState& ph, LaneCounters& cnt, Hook* hook = nullptr) {
+                                             PhotonState& ph, LaneCounters& cnt, Hook* hook = nullptr,
+                                             const DoseSink* dose = nullptr) {
   float energy = ph.energy;
   int index = __float2int_rd((energy - P.e0) * P.ide);
   float2 w = __ldg(reinterpret_cast<const float2*>(T.woodcock) + index);
@@ -135,6 +170,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
     if (randno < prob) {
       /* Compton */
       double costh;
+      const float e_before = energy;
       if (!sample_compton(rng, energy, mat0, C, rn, costh)) {
         Counting<true>::add(cnt.guard, 1);
         ph.energy = energy;
@@ -142,6 +178,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       }
       rotate(ph.dir, costh, 6.28318530717958647693 * ranecu_double(rng));
       Counting<kCount>::add(cnt.compton, 1);
+      if (dose) (*dose)(P, energy - e_before, mat0, ph.pos);
       index = __float2int_rd((energy - P.e0) * P.ide);
       if (index > -1) {
         w = __ldg(reinterpret_cast<const float2*>(T.woodcock) + index);
@@ -167,6 +204,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
         /* photoelectric absorption */
         index = -11;
         Counting<kCount>::add(cnt.photo, 1);
+        if (dose) (*dose)(P, -energy, mat0, ph.pos);
       }
     }
     if (index < 0) break;
@@ -317,6 +355,8 @@ constexpr int kBlock = 256;
 template <bool kCount>
 __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, DeviceTables T, DeviceTallies O) {
   __shared__ ComptonTable cmp;
+  __shared__ unsigned long long mdose_sh[2 * kMaxMaterials];
+  if (threadIdx.x < 2 * kMaxMaterials) mdose_sh[threadIdx.x] = 0;
   extern __shared__ float4 dyn_smem[];
   /* dynamic shared layout: [spectrum ints][palette entries][rn scratch] */
   int* spec_sh = nullptr;
@@ -348,6 +388,8 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
   LaneCounters cnt = {};
   unsigned long long histories = 0, detected = 0;
   const bool background = P.background_mode != 0;
+  const DoseSink dose{O.mat_dose ? mdose_sh : nullptr, O.vox_dose};
+  const bool dose_on = O.mat_dose || O.vox_dose;
   for (;;) {
     uint64_t lane = claim_lane(O.lane_cursor);
     if (lane >= P.n_lanes) break;
@@ -379,14 +421,14 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       a.travel = 0.0f;
       a.state = 0;
       Counting<kCount>::add(cnt.photons, 2);
-      bool esc_a = track_photon<kCount>(rng, P, T, pal, cmp, rn, a, cnt);
+      bool esc_a = track_photon<kCount>(rng, P, T, pal, cmp, rn, a, cnt, (NoStepHook*)nullptr, dose_on ? &dose : nullptr);
 
       emit_second(rng, background, dir0, b.dir);
       b.pos = origin;
       b.energy = kAnnihilation;
       b.travel = 0.0f;
       b.state = 0;
-      bool esc_b = track_photon<kCount>(rng, P, T, pal, cmp, rn, b, cnt);
+      bool esc_b = track_photon<kCount>(rng, P, T, pal, cmp, rn, b, cnt, (NoStepHook*)nullptr, dose_on ? &dose : nullptr);
 
       if (esc_a && esc_b) {
         bool pass = (P.tally_type == 0) || (P.tally_type == 1 && b.state == 0 && a.state == 0) ||
@@ -415,6 +457,8 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
   if (spec_sh)
     for (int i = threadIdx.x; i < P.ne; i += blockDim.x)
       if (spec_sh[i]) atomicAdd(&O.spectrum[i], spec_sh[i]);
+  if (O.mat_dose && threadIdx.x < 2 * kMaxMaterials && mdose_sh[threadIdx.x])
+    atomicAdd(&O.mat_dose[threadIdx.x], mdose_sh[threadIdx.x]);
 }
 
 /* ------------------------------------------------------- event kernel
@@ -467,7 +511,8 @@ struct ColdState {
 };
 
 
-template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false, bool kBatch = false, bool kRecord = false>
+template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false, bool kBatch = false, bool kRecord = false,
+          bool kDose = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(TransportParams P, DeviceTables T,
                                                                               DeviceTallies O,
                                                                               const SceneSlot* __restrict__ slots,
@@ -478,11 +523,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
    * launch's lanes are the scenes' lanes one scene after the other, and each
    * lane reads its scene's parameters, lane plan, tables and tallies from
    * slots[scene].  kRecord: tallied coincidences are also written to
-   * O.events for the gradient replay. */
+   * O.events for the gradient replay.  kDose: the material and voxel dose
+   * tallies are on (O.mat_dose / O.vox_dose, or the slots' in a batch). */
   /* kDevicePlan: the lane plan was built on the device and its size is read
    * from device memory instead of the launch parameters */
   const uint64_t n_lanes = kDevicePlan ? (uint64_t)O.plan_counts[0] : P.n_lanes;
   const int n_emitters = kDevicePlan ? (int)O.plan_counts[1] : P.n_emitters;
+  __shared__ unsigned long long mdose_sh[2 * kMaxMaterials];
   __shared__ ComptonTable cmp;
   __shared__ float s0_ann[kMaxMaterials];
   extern __shared__ float4 dyn_smem[];
@@ -514,12 +561,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   __syncthreads();
   if (threadIdx.x < kMaxMaterials)
     s0_ann[threadIdx.x] = cmp.noscco[threadIdx.x] > 0 ? compton_s0(P.e_annihilation, threadIdx.x, cmp) : 0.0f;
+  if (threadIdx.x < 2 * kMaxMaterials) mdose_sh[threadIdx.x] = 0;
   __syncthreads();
 
   LaneCounters cnt = {};
   unsigned long long histories = 0, detected = 0;
   const bool background = P.background_mode != 0;
   int scene = 0;            /* scene of the current lane (kBatch) */
+  /* dose: a block-shared copy of the material sums (global ones in a batch) */
+  const bool dose_on = kDose && (kBatch || O.mat_dose || O.vox_dose);
 
   /* hot per-thread state */
   Rng rng = {0, 0};
@@ -589,10 +639,16 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           escaped = false;
           phase = kPhEnd;
         } else {
+          const float e_before = ph.energy;
           ph.energy = e;
           rotate(ph.dir, costh, 6.28318530717958647693 * ranecu_double(rng));
           if (is_compton) {
             Counting<kCount>::add(cnt.compton, 1);
+            if (dose_on) {
+              const DoseSink ds{kBatch ? slots[scene].O.mat_dose : (O.mat_dose ? mdose_sh : nullptr),
+                                kBatch ? slots[scene].O.vox_dose : O.vox_dose};
+              ds(PS, e - e_before, mat0, ph.pos);
+            }
             index = __float2int_rd((e - PS.e0) * PS.ide);
             if (index > -1) {
               float2 w = __ldg(reinterpret_cast<const float2*>(TS.woodcock) + index);
@@ -782,6 +838,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
                     escaped = false;
                     phase = kPhEnd;
                     Counting<kCount>::add(cnt.photo, 1);
+                    if (dose_on) {
+                      const DoseSink ds{kBatch ? slots[scene].O.mat_dose : (O.mat_dose ? mdose_sh : nullptr),
+                                        kBatch ? slots[scene].O.vox_dose : O.vox_dose};
+                      ds(PS, -E, mat0, ph.pos);
+                    }
                   }
                 }
               }
@@ -817,6 +878,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   if (spec_sh)
     for (int i = threadIdx.x; i < P.ne; i += blockDim.x)
       if (spec_sh[i]) atomicAdd(&O.spectrum[i], spec_sh[i]);
+  if (kDose && !kBatch && O.mat_dose && threadIdx.x < 2 * kMaxMaterials && mdose_sh[threadIdx.x])
+    atomicAdd(&O.mat_dose[threadIdx.x], mdose_sh[threadIdx.x]);
 }
 
 /* ---------------------------------------------------------- probes */
@@ -1265,6 +1328,11 @@ static cudaError_t occupancy_of(K kernel, int block, size_t smem, int* bps) {
 constexpr int kEventBlocks = 4;
 
 cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t smem, int* blocks_per_sm) {
+  if (algorithm == kAlgorithmEventsDose)
+    return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, false, false, true>, block, smem,
+                                   blocks_per_sm)
+                    : occupancy_of(transport_events_kernel<false, kEventBlocks, false, false, false, true>, block,
+                                   smem, blocks_per_sm);
   if (algorithm == kAlgorithmEventsRecord)
     return counters
                ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, false, true>, block, smem, blocks_per_sm)
@@ -1282,7 +1350,14 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t 
 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream) {
-  if (algorithm == kAlgorithmEventsRecord) {
+  if (algorithm == kAlgorithmEventsDose) {
+    if (counters)
+      transport_events_kernel<true, kEventBlocks, false, false, false, true><<<grid, block, smem, stream>>>(P, T, O,
+                                                                                                         nullptr, 0);
+    else
+      transport_events_kernel<false, kEventBlocks, false, false, false, true><<<grid, block, smem, stream>>>(P, T, O,
+                                                                                                          nullptr, 0);
+  } else if (algorithm == kAlgorithmEventsRecord) {
     if (counters)
       transport_events_kernel<true, kEventBlocks, false, false, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
     else
@@ -1301,14 +1376,29 @@ cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, co
   return cudaGetLastError();
 }
 
-cudaError_t transport_batch_occupancy(bool counters, int block, size_t smem, int* blocks_per_sm) {
+cudaError_t transport_batch_occupancy(bool counters, bool dose, int block, size_t smem, int* blocks_per_sm) {
+  if (dose)
+    return counters
+               ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, true, false, true>, block, smem,
+                              blocks_per_sm)
+               : occupancy_of(transport_events_kernel<false, kEventBlocks, false, true, false, true>, block, smem,
+                              blocks_per_sm);
   return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, true>, block, smem, blocks_per_sm)
                   : occupancy_of(transport_events_kernel<false, kEventBlocks, false, true>, block, smem, blocks_per_sm);
 }
 
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                                   const SceneSlot* slots, int n_slots, bool counters, int grid, int block,
-                                   size_t smem, cudaStream_t stream) {
+                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int grid,
+                                   int block, size_t smem, cudaStream_t stream) {
+  if (dose) {
+    if (counters)
+      transport_events_kernel<true, kEventBlocks, false, true, false, true><<<grid, block, smem, stream>>>(P, T, O, slots,
+                                                                                                         n_slots);
+    else
+      transport_events_kernel<false, kEventBlocks, false, true, false, true><<<grid, block, smem, stream>>>(P, T, O,
+                                                                                                          slots, n_slots);
+    return cudaGetLastError();
+  }
   if (counters)
     transport_events_kernel<true, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
   else

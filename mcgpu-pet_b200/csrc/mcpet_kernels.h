@@ -12,6 +12,7 @@ constexpr int kAlgorithmHistories = 1;  /* one lane per thread, history after hi
 constexpr int kAlgorithmEvents = 2;     /* warp-regrouped event loop, registers capped for occupancy */
 constexpr int kAlgorithmEventsUncapped = 3; /* same loop, registers not capped (MCPET_MINBLOCKS=1) */
 constexpr int kAlgorithmEventsRecord = 4;   /* event loop that also records tallied coincidences (gradient) */
+constexpr int kAlgorithmEventsDose = 5;     /* event loop with the dose tallies */
 
 size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();
@@ -20,10 +21,10 @@ cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, co
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream);
 
 /* batched runs: several scenes in one launch of the event kernel */
-cudaError_t transport_batch_occupancy(bool counters, int block, size_t smem, int* blocks_per_sm);
+cudaError_t transport_batch_occupancy(bool counters, bool dose, int block, size_t smem, int* blocks_per_sm);
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                                   const SceneSlot* slots, int n_slots, bool counters, int grid, int block,
-                                   size_t smem, cudaStream_t stream);
+                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int grid,
+                                   int block, size_t smem, cudaStream_t stream);
 
 /* allocation-free runs: lane plan and work-queue words in a static device array */
 constexpr int kNoAllocMaxVoxels = 1 << 20;

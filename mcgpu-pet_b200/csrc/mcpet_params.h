@@ -95,6 +95,7 @@ struct TransportParams {
   int quorum_pair;        /* ... and a pair-bookkeeping (end of photon, next decay) round */
   int step_keep;          /* Woodcock batches continue while step_keep/8 of the stepping lanes step */
   int sino_dry;           /* 1: detector draws as usual but no sinogram, image, spectrum writes */
+  int dose_roi[6];        /* voxel dose ROI x0,x1,y0,y1,z0,z1 (0-based, clamped); x1 < 0: off */
 };
 
 /* Device pointers of one scene (all read-only during transport). */
@@ -125,6 +126,8 @@ struct DeviceTallies {
   unsigned long long* guard;      /* guard trips */
   unsigned long long* lane_cursor;/* lane work queue head */
   const unsigned long long* plan_counts; /* [lanes, emitters] on the device (device-built plans) */
+  unsigned long long* mat_dose;   /* [15][2] material dose tally, or NULL */
+  unsigned long long* vox_dose;    /* [ROI voxels][2] voxel dose tally, or NULL */
   uint32_t* events;               /* detected-coincidence records (EventRecord) for the gradient, or NULL */
   unsigned long long* event_count;
   long long event_capacity;

@@ -69,6 +69,10 @@ struct mcpet_scene {
     int ne_alloc = -1;
     void* ev0 = nullptr;
     void* ev1 = nullptr;
+    /* dose tallies: material sums [15][2], ROI voxel sums [n][2] */
+    unsigned long long* mdose = nullptr;
+    unsigned long long* vdose = nullptr;
+    long long vdose_alloc = -1;
     /* gradient (mcpet_grad): event records, device activity, small words */
     uint32_t* events = nullptr;
     long long event_cap = 0;
@@ -98,5 +102,7 @@ mcpet_status finalize_scene(mcpet_scene* sc);
 mcpet_status write_outputs(const mcpet_scene* sc, const mcpet_tallies* t, const char* out_dir, int bg,
                            double elapsed_s);
 void derive_sinogram_sizes(mcpet_config* cfg);
+long long dose_voxels(const mcpet_config& c);
+std::string format_materials_dose(const mcpet_scene* sc, const unsigned long long* md, unsigned long long n_hist);
 
 }  // namespace mcpet

@@ -101,6 +101,7 @@ class SceneInfo(C.Structure):
         ("n_emitters", C.c_int),
         ("n_lanes", C.c_longlong),
         ("last_h2d_bytes", C.c_longlong),
+        ("n_dose_voxels", C.c_longlong),
     ]
 
 
@@ -147,6 +148,8 @@ class Tallies(C.Structure):
         ("coincidences", C.c_void_p),
         ("counters", C.c_void_p),
         ("transport_ms", C.c_void_p),
+        ("material_dose", C.c_void_p),
+        ("voxel_dose", C.c_void_p),
     ]
 
 

@@ -50,6 +50,8 @@ class InputSpec:
     tally_psf_sinogram: int = 2             # 0 both, 1 PSF, 2 sinogram
     material_dose: bool = False
     voxel_dose: bool = False
+    dose_file: str = "mc-gpu_dose.dat"
+    dose_roi: Sequence[int] = (1, 1, 1, 1, 1, 1)   # 1-based x_min, x_max, y_min, y_max, z_min, z_max
     energy_resolution: float = 0.12
     energy_low: float = 350000.0
     energy_high: float = 600000.0
@@ -93,10 +95,10 @@ def write_input(path: str, s: InputSpec) -> str:
         "#[SECTION DOSE DEPOSITION v.2012-12-12]",
         f"{'YES' if s.material_dose else 'NO'}            # TALLY MATERIAL DOSE? [YES/NO]",
         f"{'YES' if s.voxel_dose else 'NO'}            # TALLY 3D VOXEL DOSE? [YES/NO]",
-        "mc-gpu_dose.dat       # OUTPUT VOXEL DOSE FILE NAME",
-        "  1  1                # VOXEL DOSE ROI: X-index min max",
-        "  1  1                # VOXEL DOSE ROI: Y-index min max",
-        "  1  1                # VOXEL DOSE ROI: Z-index min max",
+        f"{s.dose_file}       # OUTPUT VOXEL DOSE FILE NAME",
+        f"  {s.dose_roi[0]}  {s.dose_roi[1]}                # VOXEL DOSE ROI: X-index min max",
+        f"  {s.dose_roi[2]}  {s.dose_roi[3]}                # VOXEL DOSE ROI: Y-index min max",
+        f"  {s.dose_roi[4]}  {s.dose_roi[5]}                # VOXEL DOSE ROI: Z-index min max",
         "",
         "#[SECTION ENERGY PARAMETERS v.2019-04-25]",
         f"{s.energy_resolution!r}       # ENERGY RESOLUTION OF THE CRYSTALS",

@@ -65,6 +65,8 @@ class RunResult:
     transport_ms: float
     counters: dict = field(default_factory=dict)
     detected: int = 0                  # coincidences counted by the kernel
+    material_dose: Optional[np.ndarray] = None   # uint64 [15, 2]: sum Edep (eV), sum Edep^2
+    voxel_dose: Optional[np.ndarray] = None      # uint64 [n_dose_voxels, 2] over the dose ROI
 
     @property
     def coincidences(self) -> int:
@@ -128,6 +130,11 @@ class _HostRun:
         t.coincidences = C.addressof(self.det)
         t.counters = C.addressof(self.cnt)
         t.transport_ms = C.addressof(self.ms)
+        self.mdose = np.zeros((_abi.MAX_MATERIALS, 2), np.uint64) if cfg.tally_material_dose else None
+        nd = int(info.n_dose_voxels)
+        self.vdose = np.zeros((nd, 2), np.uint64) if nd > 0 else None
+        t.material_dose = _ptr(self.mdose) if self.mdose is not None else None
+        t.voxel_dose = _ptr(self.vdose) if self.vdose is not None else None
         self.t = t
 
     def result(self) -> RunResult:
@@ -135,7 +142,7 @@ class _HostRun:
         counters = {name: int(getattr(self.cnt, name)) for name, _ in _abi.Counters._fields_}
         psf = self.psf[: max(0, min(n, self.cap))] if self.psf is not None else None
         return RunResult(self.trues, self.scatter, self.img_t, self.img_s, self.spec, psf, n, int(self.hist.value),
-                         float(self.ms.value), counters, int(self.det.value))
+                         float(self.ms.value), counters, int(self.det.value), self.mdose, self.vdose)
 
 
 class Scene:
@@ -367,6 +374,10 @@ class Scene:
             t.psf_capacity = len(result.psf)
         t.psf_count = C.addressof(psf_count)
         t.total_histories = C.addressof(hist)
+        if result.material_dose is not None:
+            t.material_dose = _ptr(result.material_dose)
+        if result.voxel_dose is not None:
+            t.voxel_dose = _ptr(result.voxel_dose)
         check(lib().mcpet_write_outputs(self._h, C.byref(t), os.fsencode(out_dir) if out_dir else None,
                                         int(bool(background_mode)), result.transport_ms * 1e-3))
 

@@ -387,6 +387,31 @@ typedef struct {
 } counts;
 
 static void add_i32(int32_t* a, int v) { __atomic_fetch_add(a, v, __ATOMIC_RELAXED); }
+static void add_u64(unsigned long long* a, unsigned long long v) { __atomic_fetch_add(a, v, __ATOMIC_RELAXED); }
+
+/* Dose of one real interaction, host branch of the reference
+ * (MCGPU-PET_kernel.cu:396-410, 1593-1650, `#ifndef USING_CUDA`): `loss` is
+ * E_after - E_before (Compton) or -E (photoelectric); tallied below -0.001 eV
+ * with terms (u64)(Edep + 0.5f) and (u64)(Edep*Edep + 0.5f), SCALE_eV = 1. */
+static void tally_dose(const orc_params* p, orc_outputs* o, float loss, int mat, vec3 pos) {
+  if (!(loss < -0.001f)) return;
+  const float edep = -1.0f * loss;
+  const unsigned long long e1 = (unsigned long long)(edep * 1.0f + 0.5f);
+  const unsigned long long e2 = (unsigned long long)(edep * edep + 0.5f);
+  if (o->material_dose) {
+    add_u64(&o->material_dose[2 * mat], e1);
+    add_u64(&o->material_dose[2 * mat + 1], e2);
+  }
+  const int* r = p->dose_roi;
+  if (!o->voxel_dose || r[1] < 0) return;
+  const short x = (short)floorf(pos.x * p->inv_vx), y = (short)floorf(pos.y * p->inv_vy),
+              z = (short)floorf(pos.z * p->inv_vz);
+  if (x < r[0] || x > r[1] || y < r[2] || y > r[3] || z < r[4] || z > r[5]) return;
+  const int dx = 1 + r[1] - r[0];
+  const long long k = (long long)(x - r[0]) + (long long)(y - r[2]) * dx + (long long)(z - r[4]) * dx * (1 + r[3] - r[2]);
+  add_u64(&o->voxel_dose[2 * k], e1);
+  add_u64(&o->voxel_dose[2 * k + 1], e2);
+}
 
 static void put_record(unsigned char* rec, unsigned long long t_emit, float travel, int voxel, float energy,
                        float z, float phi, vec3 d, int state) {
@@ -482,7 +507,7 @@ static void detect(rng_t* s, const orc_params* p, orc_outputs* o, int voxel, uns
 /* Woodcock tracking and interactions of one photon (MCGPU-PET_kernel.cu:
  * 298-414); returns 1 when it leaves the voxel box, 0 when absorbed. */
 static int track(rng_t* s, const orc_params* p, const orc_tables* t, const int32_t* mat0, const float* rho,
-                 photon* ph, counts* cnt) {
+                 photon* ph, counts* cnt, orc_outputs* o) {
   float energy = ph->energy;
   int index = fl((energy - p->e0) * p->ide);
   float mfp_w = t->woodcock[2 * index] + energy * t->woodcock[2 * index + 1];
@@ -518,9 +543,11 @@ static int track(rng_t* s, const orc_params* p, const orc_tables* t, const int32
     if (v < 0) break;
     prob += md * (a[1] + energy * b[1]);
     if (u < prob) {
+      const float e_before = energy;
       double c = compton(s, &energy, mat, t);
       rotate(&ph->dir, c, 6.28318530717958647693 * ranecu_double(s));
       cnt->c[5]++;
+      tally_dose(p, o, energy - e_before, mat, ph->pos);
       index = fl((energy - p->e0) * p->ide);
       if (index > -1) {
         mfp_w = t->woodcock[2 * index] + energy * t->woodcock[2 * index + 1];
@@ -538,6 +565,7 @@ static int track(rng_t* s, const orc_params* p, const orc_tables* t, const int32
       } else {
         index = -11;
         cnt->c[7]++;
+        tally_dose(p, o, -energy, mat, ph->pos);
       }
     }
     if (index < 0) break;
@@ -571,13 +599,13 @@ static unsigned long long run_lane(const orc_params* p, const orc_tables* t, con
     a.travel = 0.f;
     a.state = 0;
     cnt->c[4] += 2;
-    int esc_a = track(&s, p, t, mat0, rho, &a, cnt);
+    int esc_a = track(&s, p, t, mat0, rho, &a, cnt, o);
     source_second(&s, p->background, d0, &b.dir);
     b.pos = origin;
     b.energy = E_ANNIHILATION;
     b.travel = 0.f;
     b.state = 0;
-    int esc_b = track(&s, p, t, mat0, rho, &b, cnt);
+    int esc_b = track(&s, p, t, mat0, rho, &b, cnt, o);
     if (esc_a && esc_b) {
       int pass = (p->tally_type == 0) || (p->tally_type == 1 && b.state == 0 && a.state == 0) ||
                  (p->tally_type == 2 && (b.state != 0 || a.state != 0));

@@ -34,6 +34,7 @@ typedef struct {
   int nrows, ncrystals, nangles, nrad, nzs, ne, mrd, span, nsinos;
   long long nbins;
   int tpb, seed, background;
+  int dose_roi[6];             /* voxel dose ROI x0,x1,y0,y1,z0,z1 (0-based); x1 < 0: off */
 } orc_params;
 
 typedef struct {
@@ -66,6 +67,8 @@ typedef struct {
    * majorant refreshes, int32 tally increments, photons, compton, rayleigh,
    * photoelectric, lanes */
   unsigned long long counters[9];
+  unsigned long long* material_dose;   /* [15][2] or NULL (tally_materials_dose) */
+  unsigned long long* voxel_dose;      /* [ROI voxels][2] or NULL (tally_voxel_energy_deposition) */
 } orc_outputs;
 
 /* Full transport over the reference lanes (tpb lanes per voxel with

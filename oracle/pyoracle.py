@@ -34,6 +34,7 @@ class Params(C.Structure):
         ("ne", C.c_int), ("mrd", C.c_int), ("span", C.c_int), ("nsinos", C.c_int),
         ("nbins", C.c_longlong),
         ("tpb", C.c_int), ("seed", C.c_int), ("background", C.c_int),
+        ("dose_roi", C.c_int * 6),
     ]
 
 
@@ -45,7 +46,7 @@ class Tables(C.Structure):
 class Outputs(C.Structure):
     _fields_ = [("trues", P), ("scatter", P), ("image_trues", P), ("image_scatter", P), ("spectrum", P),
                 ("psf", P), ("psf_count", C.c_int32), ("histories", C.c_ulonglong),
-                ("counters", C.c_ulonglong * 9)]
+                ("counters", C.c_ulonglong * 9), ("material_dose", P), ("voxel_dose", P)]
 
 
 COUNTER_NAMES = ["woodcock_steps_inside", "table_refreshes", "majorant_refreshes", "tally_increments", "photons",
@@ -106,6 +107,11 @@ class OracleScene:
         p.tpb = cfg.threads_per_block
         p.seed = cfg.seed if seed is None else seed
         p.background = int(bool(background))
+        roi = list(cfg.dose_roi) if cfg.tally_voxel_dose else [0, -1, 0, -1, 0, -1]
+        for k in range(6):
+            p.dose_roi[k] = int(roi[k])
+        self.material_dose = bool(cfg.tally_material_dose)
+        self.n_dose = int(info.n_dose_voxels)
         self.p = p
         self._tab = Tables()
         for n, _ in Tables._fields_:
@@ -128,6 +134,9 @@ class OracleScene:
         for k in ["trues", "scatter", "image_trues", "image_scatter", "spectrum"]:
             setattr(o, k, _p(out[k]))
         o.psf = _p(psf)
+        md = np.zeros((M, 2), np.uint64) if self.material_dose else None
+        vd = np.zeros((self.n_dose, 2), np.uint64) if self.n_dose > 0 else None
+        o.material_dose, o.voxel_dose = _p(md), _p(vd)
         vl = None if voxel_list is None else np.ascontiguousarray(voxel_list, np.int32)
         rc = lib().orc_run(C.byref(p), C.byref(self._tab), _p(self.mat0), _p(self.rho), _p(self.act), _p(vl),
                            0 if vl is None else len(vl), int(n_threads), C.byref(o))
@@ -137,6 +146,7 @@ class OracleScene:
         n = max(0, min(o.psf_count, p.psf_capacity))
         out["psf_raw"] = None if psf is None else psf[: n * 44]
         out["counters"] = {k: int(o.counters[i]) for i, k in enumerate(COUNTER_NAMES)}
+        out["material_dose"], out["voxel_dose"] = md, vd
         return out
 
 

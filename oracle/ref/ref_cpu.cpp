@@ -73,33 +73,43 @@ static void fill_structs(const refc_params* p, detector_struct* d, source_struct
   s->acquisition_time_ps = p->acq_ps; s->mean_life = p->mean_life;
 }
 
-static void set_constants(const refc_params* p) {
+static void set_constants(const refc_params* p, const short* roi) {
   voxel_data_CONST.num_voxels.x = p->nx; voxel_data_CONST.num_voxels.y = p->ny; voxel_data_CONST.num_voxels.z = p->nz;
   voxel_data_CONST.inv_voxel_size.x = p->inv_vx; voxel_data_CONST.inv_voxel_size.y = p->inv_vy;
   voxel_data_CONST.inv_voxel_size.z = p->inv_vz;
   voxel_data_CONST.size_bbox.x = p->bbx; voxel_data_CONST.size_bbox.y = p->bby; voxel_data_CONST.size_bbox.z = p->bbz;
   mfp_table_data_CONST.num_values = p->n_e; mfp_table_data_CONST.e0 = p->e0; mfp_table_data_CONST.ide = p->ide;
-  dose_ROI_x_min_CONST = 32500; dose_ROI_x_max_CONST = -32500;
-  dose_ROI_y_min_CONST = 32500; dose_ROI_y_max_CONST = -32500;
-  dose_ROI_z_min_CONST = 32500; dose_ROI_z_max_CONST = -32500;
+  if (roi) {
+    dose_ROI_x_min_CONST = roi[0]; dose_ROI_x_max_CONST = roi[1];
+    dose_ROI_y_min_CONST = roi[2]; dose_ROI_y_max_CONST = roi[3];
+    dose_ROI_z_min_CONST = roi[4]; dose_ROI_z_max_CONST = roi[5];
+  } else {
+    dose_ROI_x_min_CONST = 32500; dose_ROI_x_max_CONST = -32500;
+    dose_ROI_y_min_CONST = 32500; dose_ROI_y_max_CONST = -32500;
+    dose_ROI_z_min_CONST = 32500; dose_ROI_z_max_CONST = -32500;
+  }
   PETA_DEV[0] = (unsigned int)p->peta; PETA_DEV[1] = 0;
 }
 
-/* Full transport over all voxel blocks (or the listed subset).
+/* Full transport over all voxel blocks (or the listed subset), with the
+ * reference's dose tallies when mat_dose (ulonglong2[15]) / vox_dose
+ * (ulonglong2[ROI voxels], roi = x0,x1,y0,y1,z0,z1) are given: its host
+ * branch adds to them without atomics, so use n_threads = 1 then.
  * Returns 0 on success. */
-int refc_run(const refc_params* p, const float* voxels /* float3[nvox] */,
-             const float* woodcock /* float2[n_e] */, const float* mfp_a, const float* mfp_b,
-             const refc_tables* tab,
-             int* trues, int* scatter, int* img_t, int* img_s, int* spectrum,
-             void* psf, int* index_psf, unsigned long long* total_histories,
-             const int* block_list, long long n_block_list, int n_threads) {
+int refc_run2(const refc_params* p, const float* voxels /* float3[nvox] */,
+              const float* woodcock /* float2[n_e] */, const float* mfp_a, const float* mfp_b,
+              const refc_tables* tab,
+              int* trues, int* scatter, int* img_t, int* img_s, int* spectrum,
+              void* psf, int* index_psf, unsigned long long* total_histories,
+              const int* block_list, long long n_block_list, int n_threads,
+              unsigned long long* mat_dose, unsigned long long* vox_dose, const short* roi) {
   compton_struct* cmp = (compton_struct*)calloc(1, sizeof(compton_struct));
   rayleigh_struct* ray = (rayleigh_struct*)calloc(1, sizeof(rayleigh_struct));
   if (!cmp || !ray) { free(cmp); free(ray); return -1; }
   fill_tables(tab, cmp, ray);
   detector_struct det; source_struct src;
   fill_structs(p, &det, &src);
-  set_constants(p);
+  set_constants(p, vox_dose ? roi : nullptr);
   const long long nvox = (long long)p->nx * p->ny * p->nz;
   const long long nb = block_list ? n_block_list : nvox;
   unsigned long long hist = 0;
@@ -118,9 +128,9 @@ int refc_run(const refc_params* p, const float* voxels /* float3[nvox] */,
       for (int t = 0; t < p->tpb; ++t) {
         threadIdx.x = t; threadIdx.y = 0; threadIdx.z = 0;
         int seed_copy = p->seed;   /* the kernel's last thread overwrites it (MCGPU-PET_kernel.cu:454) */
-        track_particles(&hist, &seed_copy, (PSF_element_struct*)psf, &idx_psf, NULL,
+        track_particles(&hist, &seed_copy, (PSF_element_struct*)psf, &idx_psf, (ulonglong2*)vox_dose,
                         (float3*)voxels, (float2*)woodcock, (float3*)mfp_a, (float3*)mfp_b,
-                        ray, cmp, &det, &src, NULL,
+                        ray, cmp, &det, &src, (ulonglong2*)mat_dose,
                         trues, scatter, img_t, img_s, spectrum,
                         p->e_resol, p->e_low, p->e_high, p->fovz, p->nrows, p->ncrystals,
                         p->nangles, p->nrad, p->nzs, p->nbins, p->res, p->nvoxs, p->ne,
@@ -132,6 +142,14 @@ int refc_run(const refc_params* p, const float* voxels /* float3[nvox] */,
   *index_psf = idx_psf;
   free(cmp); free(ray);
   return 0;
+}
+
+int refc_run(const refc_params* p, const float* voxels, const float* woodcock, const float* mfp_a,
+             const float* mfp_b, const refc_tables* tab, int* trues, int* scatter, int* img_t, int* img_s,
+             int* spectrum, void* psf, int* index_psf, unsigned long long* total_histories, const int* block_list,
+             long long n_block_list, int n_threads) {
+  return refc_run2(p, voxels, woodcock, mfp_a, mfp_b, tab, trues, scatter, img_t, img_s, spectrum, psf, index_psf,
+                   total_histories, block_list, n_block_list, n_threads, nullptr, nullptr, nullptr);
 }
 
 /* RANECU jump-ahead and first draws (MCGPU-PET_kernel.cu:925-1083). */

@@ -170,6 +170,11 @@ typedef struct {
   unsigned long long total_histories;
   float kernel_ms;       /* track_particles, CUDA events */
   int nbins, nvox, ne;
+  unsigned long long* material_dose;   /* ulonglong2[15] or NULL */
+  unsigned long long* voxel_dose;      /* ulonglong2[voxel_dose_capacity] or NULL */
+  long long voxel_dose_capacity;
+  short roi[6];                        /* the ROI as the reference used it (after load_voxels' clipping) */
+  long long n_roi;                     /* voxels of that ROI (0 when the voxel tally is off) */
 } refp_outputs;
 
 #define PCHK(x)                                                                        \
@@ -301,6 +306,15 @@ int refp_run(const char* in_path, int bg, refp_outputs* out) {
   if (out->image_scatter)
     PCHK(cudaMemcpy(out->image_scatter, Imagen_SC_dev, (size_t)NVOX_SIM * 4, cudaMemcpyDeviceToHost));
   if (out->spectrum) PCHK(cudaMemcpy(out->spectrum, Energy_Spectrum_dev, (size_t)NE * 4, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 6; ++k) out->roi[k] = roi[k];
+  out->n_roi = roi[1] > -1 ? (long long)(roi[1] - roi[0] + 1) * (roi[3] - roi[2] + 1) * (roi[5] - roi[4] + 1) : 0;
+  if (out->material_dose && flag_material_dose == 1)
+    PCHK(cudaMemcpy(out->material_dose, materials_dose_device, MAX_MATERIALS * sizeof(ulonglong2),
+                    cudaMemcpyDeviceToHost));
+  if (out->voxel_dose && out->n_roi > 0 && voxels_Edep_device) {
+    long long n = out->n_roi < out->voxel_dose_capacity ? out->n_roi : out->voxel_dose_capacity;
+    PCHK(cudaMemcpy(out->voxel_dose, voxels_Edep_device, (size_t)n * sizeof(ulonglong2), cudaMemcpyDeviceToHost));
+  }
   if (out->psf && out->psf_capacity > 0) {
     long long n = index_PSF < detector_data.PSF_size ? index_PSF : detector_data.PSF_size;
     if (n > out->psf_capacity) n = out->psf_capacity;

@@ -198,6 +198,8 @@ class RefCPU:
         self.L = C.CDLL(os.path.join(REF_DIR, "libref_cpu.so"))
         self.L.refc_run.argtypes = [P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, C.c_longlong, C.c_int]
         self.L.refc_run.restype = C.c_int
+        self.L.refc_run2.argtypes = self.L.refc_run.argtypes + [P, P, P]
+        self.L.refc_run2.restype = C.c_int
         self.L.refc_prng.argtypes = [C.c_int, C.c_int, P, C.c_int, P, P, P]
         self.L.refc_sinogram_events.argtypes = [P, C.c_int] + [P] * 15
         self.L.refc_gcoa.argtypes = [C.c_int, P, P, P, P, P, P, P]
@@ -206,7 +208,9 @@ class RefCPU:
         self.L.refc_abmodm.restype = C.c_int
 
     def run(self, p: Params, voxels: np.ndarray, t: RefTables, block_list=None, n_threads: int = 0,
-            psf_capacity: int = 0):
+            psf_capacity: int = 0, material_dose: bool = False, dose_roi=None):
+        """dose_roi: 0-based (x0, x1, y0, y1, z0, z1) enables the voxel dose tally;
+        the reference's host dose tallies are not atomic, so n_threads must be 1."""
         nv = p.nx * p.ny * p.nz
         out = {
             "trues": np.zeros(p.nbins, np.int32), "scatter": np.zeros(p.nbins, np.int32),
@@ -220,12 +224,21 @@ class RefCPU:
         bl = None if block_list is None else np.ascontiguousarray(block_list, np.int32)
         p2 = Params.from_buffer_copy(p)
         p2.psf_size = psf_capacity
-        rc = self.L.refc_run(C.byref(p2), _p(np.ascontiguousarray(voxels, np.float32)), _p(t.woodcock),
-                             _p(t.mfp_a), _p(t.mfp_b), C.byref(tab), _p(out["trues"]), _p(out["scatter"]),
-                             _p(out["image_trues"]), _p(out["image_scatter"]), _p(out["spectrum"]), _p(psf),
-                             C.addressof(idx), C.addressof(hist), _p(bl), 0 if bl is None else len(bl),
-                             int(n_threads))
+        md = np.zeros((15, 2), np.uint64) if material_dose else None
+        vd, roi = None, None
+        if dose_roi is not None:
+            roi = np.ascontiguousarray(dose_roi, np.int16)
+            nd = int(roi[1] - roi[0] + 1) * int(roi[3] - roi[2] + 1) * int(roi[5] - roi[4] + 1)
+            vd = np.zeros((nd, 2), np.uint64)
+        if (md is not None or vd is not None) and n_threads != 1:
+            raise ValueError("the reference's host dose tallies need n_threads=1")
+        rc = self.L.refc_run2(C.byref(p2), _p(np.ascontiguousarray(voxels, np.float32)), _p(t.woodcock),
+                              _p(t.mfp_a), _p(t.mfp_b), C.byref(tab), _p(out["trues"]), _p(out["scatter"]),
+                              _p(out["image_trues"]), _p(out["image_scatter"]), _p(out["spectrum"]), _p(psf),
+                              C.addressof(idx), C.addressof(hist), _p(bl), 0 if bl is None else len(bl),
+                              int(n_threads), _p(md), _p(vd), _p(roi))
         assert rc == 0
+        out["material_dose"], out["voxel_dose"] = md, vd
         out["psf_count"] = idx.value
         out["total_histories"] = hist.value
         n = max(0, min(idx.value, psf_capacity))
@@ -291,7 +304,8 @@ class ProgOutputs(C.Structure):
     _fields_ = [("trues", P), ("scatter", P), ("image_trues", P), ("image_scatter", P), ("spectrum", P),
                 ("psf", P), ("psf_capacity", C.c_longlong), ("psf_count", C.c_int),
                 ("total_histories", C.c_ulonglong), ("kernel_ms", C.c_float), ("nbins", C.c_int),
-                ("nvox", C.c_int), ("ne", C.c_int)]
+                ("nvox", C.c_int), ("ne", C.c_int), ("material_dose", P), ("voxel_dose", P),
+                ("voxel_dose_capacity", C.c_longlong), ("roi", C.c_short * 6), ("n_roi", C.c_longlong)]
 
 
 class RefProg:
@@ -303,7 +317,7 @@ class RefProg:
         self.L.refp_run.restype = C.c_int
 
     def run(self, in_path: str, nbins: int, nvox: int, ne: int, background: bool = False, psf_capacity: int = 0,
-            cwd: Optional[str] = None) -> dict:
+            cwd: Optional[str] = None, dose_voxels: int = 0) -> dict:
         out = {"trues": np.zeros(nbins, np.int32), "scatter": np.zeros(nbins, np.int32),
                "image_trues": np.zeros(nvox, np.int32), "image_scatter": np.zeros(nvox, np.int32),
                "spectrum": np.zeros(max(ne, 1), np.int32)}
@@ -313,6 +327,10 @@ class RefProg:
             setattr(o, k, _p(out[k]))
         o.psf = _p(psf)
         o.psf_capacity = psf_capacity
+        md = np.zeros((15, 2), np.uint64)
+        vd = np.zeros((max(dose_voxels, 1), 2), np.uint64)
+        o.material_dose, o.voxel_dose, o.voxel_dose_capacity = _p(md), _p(vd), dose_voxels
+        out["material_dose"], out["voxel_dose"] = md, vd[:dose_voxels]
         with _chdir(cwd):
             rc = _quiet_call(self.L.refp_run, os.fsencode(in_path), int(bool(background)), C.byref(o))
         if rc != 0:
@@ -321,6 +339,8 @@ class RefProg:
         out["psf_count"] = o.psf_count
         out["total_histories"] = int(o.total_histories)
         out["kernel_ms"] = float(o.kernel_ms)
+        out["roi"] = [int(v) for v in o.roi]
+        out["n_roi"] = int(o.n_roi)
         n = max(0, min(o.psf_count, psf_capacity))
         out["psf_raw"] = psf[: n * 44]
         return out

@@ -119,3 +119,23 @@ def test_pin_rng_and_probes(workdir):
     ev = scenes.random_events(5000, np.random.default_rng(11))
     p = refbind.params_from_scene(sc)
     np.testing.assert_array_equal(pyoracle.detector(osc, ev), ref.sinogram_events(p, ev))
+
+
+def test_pin_dose_tallies(workdir):
+    """Material and ROI voxel dose (tally_materials_dose, tally_voxel_energy_deposition):
+    the oracle's sums equal the reference host build's, term by term rounding included;
+    the ROI's upper corner beyond the phantom is clipped as load_voxels does."""
+    sc = scenes.sample_scene(workdir, material_dose=True, voxel_dose=True, dose_roi=(2, 8, 1, 9, 4, 99), seed=777)
+    cfg, info = sc.config, sc.info
+    assert list(cfg.dose_roi) == [1, 7, 0, 8, 3, 8]          # 0-based, z clipped to the 9-voxel phantom
+    assert info.n_dose_voxels == 7 * 9 * 6
+    osc = pyoracle.OracleScene(sc)
+    o = osc.run(n_threads=4)
+    p = refbind.params_from_scene(sc, peta=1)
+    r = refbind.RefCPU().run(p, osc.t["voxels"], refbind.RefTables.from_scene_export(osc.t), n_threads=1,
+                             material_dose=True, dose_roi=list(cfg.dose_roi))
+    _assert_same(o, r)
+    assert o["material_dose"][:, 0].sum() > 0 and o["voxel_dose"][:, 0].sum() > 0
+    np.testing.assert_array_equal(o["material_dose"], r["material_dose"])
+    np.testing.assert_array_equal(o["voxel_dose"], r["voxel_dose"])
+    sc.close()
