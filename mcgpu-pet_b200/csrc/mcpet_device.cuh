@@ -316,6 +316,8 @@ __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, c
         if (pz > 0.0f) t = 1.0f - t;
         s += C.fco[mat + i * kMaxMaterials] * t;
         rn[i] = t;
+      } else {
+        rn[i] = 0.0f;   /* shell above the photon energy: the reference leaves it uninitialised */
       }
     }
     if (!((ranecu(r) * s0) >

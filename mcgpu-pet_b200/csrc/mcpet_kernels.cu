@@ -1310,9 +1310,8 @@ static cudaError_t occupancy_smem_attr(K kernel, size_t smem) {
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  if (smem > 48 * 1024)
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return cudaSuccess;
+  /* static + dynamic above 48 KB needs the opt-in, so always state the size */
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 template <typename K>

@@ -281,6 +281,8 @@ static double compton(rng_t* s, float* energy, int mat, const orc_tables* t) {
         if (pz > 0.0f) q = 1.0f - q;
         sv += t->fco[mat + i * NM] * q;
         rn[i] = q;
+      } else {
+        rn[i] = 0.0f;   /* shell above the photon energy: the reference leaves it uninitialised */
       }
     }
     if (!((ranecu(s) * s0) > (sv * (1.0f + tau * ((ek3 - ek2 - 1.0f) + tau * (ek2 + tau * ek3)))) /
