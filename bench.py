@@ -193,11 +193,20 @@ def run_reference_arm(args):
     return 0
 
 
-def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8) -> dict:
-    """Batched many-phantom workload: one mcpet_run_batch launch against the
-    same scenes run one after another (mcpet_run), same options and seeds.
-    Both give identical tallies; times are the transport kernels' (CUDA
-    events) and the wall clock of the host calls."""
+def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, replays: int = 3) -> dict:
+    """Batched many-phantom workload (config C3 shapes): n_scenes head-like
+    phantoms of uneven size, each its own seed.  Device-resident tallies
+    throughout; times are CUDA events on the launch stream.
+
+    * sequential: the scenes one after another through mcpet_run_device
+      (one launch each), the plain form of the run;
+    * batched: one mcpet_run_batch_device launch over all scenes;
+    * autotuned: mcpet_autotune picks histories per lane and block size on a
+      sample, then the batched launch with that choice;
+    * graph: the tuned batch captured once (mcpet_batch_graph_create) and
+      replayed; every replay regenerates all histories with new seeds.
+    Also checks that the batched tallies equal the sequential ones."""
+    import torch
     import mcpet
     from mcpet import inputs
     sc, sizes = [], []
@@ -207,31 +216,74 @@ def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8) ->
         cfg = inputs.config_from_spec(spec, workdir)
         sc.append(mcpet.Scene.from_arrays(cfg, mat, rho, act, vs))
         sizes.append(mat.shape[0])
-    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED)
-    for s in sc:                                  # warm-up: device tables, run buffers
-        s.run(opts)
-    mcpet.Scene.run_batch(sc, opts)
+    tal = [mcpet.device_tallies_for(s) for s in sc]
+    stream = torch.cuda.current_stream()
+    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED, stream=stream.cuda_stream)
+
+    def coinc():
+        return sum(int(t["coincidences"].item()) for t in tal)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), time.perf_counter() - t0
+
+    for s, t in zip(sc, tal):                     # warm-up: device tables, lane plans
+        s.run_device(t, opts)
+    mcpet.Scene.run_batch_device(sc, tal, opts)
+
+    seq_ms, seq_wall = timed(lambda: [s.run_device(t, opts) for s, t in zip(sc, tal)])
+    seq_c = coinc()
+    seq_trues = [t["trues"].clone() for t in tal[:4]]
+    bat_ms, bat_wall = timed(lambda: mcpet.Scene.run_batch_device(sc, tal, opts))
+    bat_c = coinc()
+    identical = bat_c == seq_c and all(bool(torch.equal(a, t["trues"])) for a, t in zip(seq_trues, tal[:4]))
+
     t0 = time.perf_counter()
-    seq = [s.run(opts) for s in sc]
-    seq_wall = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    bat = mcpet.Scene.run_batch(sc, opts)
-    bat_wall = time.perf_counter() - t0
-    coinc = sum(r.detected for r in bat)
-    identical = all(a.detected == b.detected and a.total_histories == b.total_histories and
-                    bool((a.trues == b.trues).all()) for a, b in zip(seq, bat))
-    seq_ms = sum(r.transport_ms for r in seq)
-    bat_ms = bat[0].transport_ms
+    tuned, tune = mcpet.autotune(sc, tal, opts, sample_decays=2.0e8 * max(1.0, n_scenes / 8))
+    tune["wall_s"] = time.perf_counter() - t0
+    mcpet.Scene.run_batch_device(sc, tal, tuned)
+    tun_ms, tun_wall = timed(lambda: mcpet.Scene.run_batch_device(sc, tal, tuned))
+    tun_c = coinc()
+    for s, t in zip(sc, tal):
+        s.run_device(t, tuned)
+    seqt_ms, seqt_wall = timed(lambda: [s.run_device(t, tuned) for s, t in zip(sc, tal)])
+    seqt_c = coinc()
+
+    g = mcpet.BatchGraph(sc, tal, tuned, seed_step=1)
+    g.launch(stream.cuda_stream)                 # warm-up replay
+    graph_c = 0
+    graph_ms, graph_wall = 0.0, 0.0
+    for _ in range(replays):
+        ms, wall = timed(lambda: g.launch(stream.cuda_stream))
+        graph_ms += ms
+        graph_wall += wall
+        graph_c += coinc()
+    guard = g.guard_trips()
+    g.close()
     for s in sc:
         s.close()
+    rate = lambda c, ms: c / (ms * 1e-3)
     return {"workload": f"{n_scenes} head-like phantoms of m^3 voxels, m in [32,192] (min {min(sizes)}, max "
-                        f"{max(sizes)}), 2-4 mm voxels, {emissions_each:.0e} decays each; scanner 32 rings, "
-                        "128 rad x 128 ang x 1985 planes (span 1)",
-            "coincidences": coinc, "identical_to_sequential": identical,
-            "batched_kernel_ms": bat_ms, "sequential_kernel_ms": seq_ms,
-            "batched_value": coinc / (bat_ms * 1e-3), "sequential_value": coinc / (seq_ms * 1e-3),
-            "batched_wall_s": bat_wall, "sequential_wall_s": seq_wall,
-            "kernel_speedup": seq_ms / bat_ms, "wall_speedup": seq_wall / bat_wall, "unit": UNIT}
+                        f"{max(sizes)}), 2-4 mm voxels, {emissions_each:.0e} decays each, own seed each; scanner "
+                        "32 rings, 128 rad x 128 ang x 1985 planes (span 1); device-resident tallies",
+            "unit": UNIT, "identical_to_sequential": identical,
+            "sequential": {"ms": seq_ms, "wall_s": seq_wall, "value": rate(seq_c, seq_ms), "launches": n_scenes},
+            "batched": {"ms": bat_ms, "wall_s": bat_wall, "value": rate(bat_c, bat_ms), "launches": 1},
+            "sequential_tuned": {"ms": seqt_ms, "wall_s": seqt_wall, "value": rate(seqt_c, seqt_ms),
+                                 "launches": n_scenes},
+            "autotune": tune,
+            "batched_tuned": {"ms": tun_ms, "wall_s": tun_wall, "value": rate(tun_c, tun_ms),
+                              "histories_per_lane": tuned.histories_per_lane, "block_threads": tuned.block_threads},
+            "graph": {"replays": replays, "ms_per_replay": graph_ms / replays, "wall_s_per_replay": graph_wall / replays,
+                      "value": rate(graph_c, graph_ms), "guard_trips": guard},
+            "graph_vs_sequential": rate(graph_c, graph_ms) / rate(seq_c, seq_ms),
+            "batched_vs_sequential": rate(bat_c, bat_ms) / rate(seq_c, seq_ms)}
 
 
 def measure_gradient(workdir: str, emissions: float = 2.0e8) -> dict:
@@ -294,6 +346,8 @@ def main():
                          "launch against the same runs one by one (reported under 'batch')")
     ap.add_argument("--batch-emissions", type=float, default=1.0e8, help="decays per phantom of --batch-scenes")
     ap.add_argument("--no-gradient", action="store_true", help="skip the gradient (mcpet_grad) measurement")
+    ap.add_argument("--block-threads", type=int, default=0, help="threads per block (0: automatic)")
+    ap.add_argument("--histories-per-lane", type=int, default=0, help="balanced lanes: decays per lane (0: automatic)")
     ap.add_argument("--scanner", default="head", choices=["head", "head32"],
                     help="head32: smaller sinogram for profiler captures (not a bench line)")
     args = ap.parse_args()
@@ -340,7 +394,8 @@ def main():
 
     def opts(step, counters=False):
         return mcpet.RunOptions(lane_mode=lanes, seed_override=base_seed + step, collect_counters=counters,
-                                stream=stream.cuda_stream, algorithm=algorithm)
+                                stream=stream.cuda_stream, algorithm=algorithm, block_threads=args.block_threads,
+                                histories_per_lane=args.histories_per_lane)
 
     # algorithmic-byte counters of one launch (separate, untimed, same seed as step 0)
     scene.run_device(tallies, opts(0, counters=True))
@@ -399,7 +454,8 @@ def main():
             t0 = time.perf_counter()
             scene.set_activity(act_pinned.numpy())
             r = scene.run_into(pin, mcpet.RunOptions(lane_mode=lanes, seed_override=base_seed + 500 + k,
-                                                     algorithm=algorithm))
+                                                     algorithm=algorithm, block_threads=args.block_threads,
+                                                     histories_per_lane=args.histories_per_lane))
             dt = time.perf_counter() - t0
             if k > 0:    # first pass warms the host plan builder
                 e2e_coinc += r["coincidences"]
@@ -450,6 +506,8 @@ def main():
                 "data": "synthetic (seeded head phantom; tissue densities on the reference's own air/water material tables)",
                 "config": {"workload": WORKLOAD, "emissions_per_step_per_gpu": args.emissions,
                            "lanes": args.lanes, "algorithm": args.algorithm, "parallelism": f"replicas x{world}",
+                           "block_threads": args.block_threads or "auto",
+                           "histories_per_lane": args.histories_per_lane or "auto",
                            "l2": "each step zeroes 4.2 GB of sinograms (> 126 MB L2) before the kernel",
                            "coincidences_per_step": total / args.steps / world, "histories_last_step": hist,
                            "guard_trips": guard},

@@ -300,6 +300,63 @@ mcpet_status mcpet_grad(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_ta
 mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                                     mcpet_tallies* device_outs);
 
+/* ---- autotuner ----------------------------------------------------------
+ *
+ * Picks histories_per_lane (balanced lanes) and block_threads for a workload
+ * of one or more scenes by timing candidates on a sample of it: every scene
+ * runs with its acquisition time scaled by f and each candidate's histories
+ * per lane scaled by f, so the sample has the workload's lanes with f of its
+ * decays (f = sample_decays / total decays, raised so that every candidate
+ * keeps at least one decay per lane; sample_decays <= 0 means 2e8).
+ * Candidates: 1/4, 1/2, 1, 2 and 4 times the automatic histories per lane of
+ * the largest scene at the full block, then smaller blocks at the best of
+ * those.  Runs go through mcpet_run_device (one scene) or
+ * mcpet_run_batch_device (several) with opts and overwrite device_outs.  The
+ * scenes' own settings are restored.  The result goes into
+ * opts->histories_per_lane / block_threads of later runs; with reference
+ * lanes only the block size is tuned. */
+typedef struct {
+  int block_threads;              /* chosen threads per block */
+  int histories_per_lane;         /* chosen expected decays per lane (0 with reference lanes) */
+  double best_ms;                 /* kernel time of the chosen pair on the sample */
+  double auto_ms;                 /* kernel time of the automatic choice on the sample */
+  double sample_fraction;         /* f */
+  int candidates;                 /* pairs timed */
+} mcpet_tune_result;
+
+mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                            const mcpet_tallies* device_outs, double sample_decays, mcpet_tune_result* out);
+
+/* ---- batched regeneration captured in a CUDA graph --------------------
+ *
+ * Repeated runs of the same scenes (iterative reconstruction, Monte Carlo
+ * averaging over seeds) need new histories every time, not new parameters.
+ * mcpet_batch_graph_create builds the batch once, as mcpet_run_batch_device
+ * does (the lane plans, the union tables, one launch of the event kernel over
+ * every scene's lanes), keeps its own copies of the lane plans and tables on
+ * the device, and captures into one CUDA graph: the zeroing of
+ * device_outs[k], the transport launch, and a step of every scene's seed.
+ * Each mcpet_batch_graph_launch then regenerates all histories with one graph
+ * launch and no host work: launch r (counted from 0, or from the last
+ * mcpet_batch_graph_set_seeds) runs scene k with seed s_k + r*seed_step
+ * (kept in [1, 2147483562]) and leaves in device_outs[k] the tallies of
+ * mcpet_run_device of scene k alone with that seed and the same options.
+ * s_k is opts->seed_override when set, else the scene's own seed.  The
+ * scenes must stay alive and on their device while the graph exists; runs of
+ * the scenes themselves do not disturb it.  Replaces repeated runs of the
+ * reference program, one phantom per process (MCGPU-PET.cu:77-840). */
+typedef struct mcpet_batch_graph mcpet_batch_graph;
+
+mcpet_status mcpet_batch_graph_create(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                                      const mcpet_tallies* device_outs, int seed_step, mcpet_batch_graph** out);
+/* One replay, ordered on `stream` (a cudaStream_t; NULL = default stream). */
+mcpet_status mcpet_batch_graph_launch(mcpet_batch_graph* graph, void* stream);
+/* Seeds of the next launch, one per scene (ordered on `stream`, blocking). */
+mcpet_status mcpet_batch_graph_set_seeds(mcpet_batch_graph* graph, const int* seeds, void* stream);
+/* Guard trips of the last completed launch (blocking read). */
+mcpet_status mcpet_batch_graph_guard_trips(mcpet_batch_graph* graph, unsigned long long* trips);
+void mcpet_batch_graph_destroy(mcpet_batch_graph* graph);
+
 /* Allocation-free variant of mcpet_run_device, for callers that may not
  * allocate device memory while they run: plugin or custom-call hooks inside a
  * host framework that hands out every device buffer from its own pool, and

@@ -2,11 +2,13 @@
  * runs and verification probes. */
 #include <cuda_runtime_api.h>
 #include <math.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -129,7 +131,8 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
     if (sc->material_loaded[m] && sc->compton.noscco[m] > ms) ms = sc->compton.noscco[m];
   P.max_shells = ms;
   P.spectrum_in_shared = (c.n_energy_bins > 0 && c.n_energy_bins <= kSpectrumSharedMax) ? 1 : 0;
-  P.palette_in_shared = (sc->palette.size() <= 2048) ? (int)sc->palette.size() : 0;
+  P.palette_in_shared =
+      (sc->palette.size() <= 2048 && env_int("MCPET_PALETTE_SHARED", 1, 0, 1)) ? (int)sc->palette.size() : 0;
   P.e_annihilation = 510998.95f;
   for (int k = 0; k < 6; ++k) P.dose_roi[k] = c.tally_voxel_dose ? c.dose_roi[k] : (k % 2 ? -1 : 0);
   P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 16, 1, 32);
@@ -319,10 +322,10 @@ mcpet_status validate_opts(const mcpet_scene* sc, const mcpet_run_opts* opts) {
   return MCPET_OK;
 }
 
-/* Parameters of one scene's run and its zeroed outputs: everything but the
- * lane plan and the launch.  O.coincidences defaults to a scene word. */
-mcpet_status prepare_run(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies& O, cudaStream_t st,
-                         TransportParams& P) {
+/* Parameters of one scene's run (host only): everything but the lane plan,
+ * the zeroing of the outputs and the launch.  O.coincidences defaults to a
+ * scene word. */
+mcpet_status prepare_params(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies& O, TransportParams& P) {
   fill_params(sc, P);
   if (o.seed_override != 0) P.seed = o.seed_override;
   if (P.seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", P.seed);
@@ -333,7 +336,16 @@ mcpet_status prepare_run(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies
   if (sino && (!O.trues || !O.scatter || !O.image_trues || !O.image_scatter || !O.spectrum))
     return set_error(MCPET_ERR_ARG, "sinogram tally requested but a sinogram/image/spectrum buffer is missing");
   if (!O.histories || !O.psf_count) return set_error(MCPET_ERR_ARG, "histories and psf_count are required");
+  if (!O.coincidences) O.coincidences = sc->dev.small + 14;
+  if (!sc->cfg.tally_material_dose) O.mat_dose = nullptr;
+  if (dose_voxels(sc->cfg) == 0) O.vox_dose = nullptr;
+  /* the kernel only touches the spectrum when the sinogram is tallied */
+  if (!sino) P.spectrum_in_shared = 0;
+  return MCPET_OK;
+}
 
+/* Zero the outputs of a prepared run, ordered on st. */
+mcpet_status zero_outputs(const mcpet_scene* sc, const DeviceTallies& O, cudaStream_t st) {
   const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
   if (O.trues) CUDA_TRY(cudaMemsetAsync(O.trues, 0, nb, st));
   if (O.scatter) CUDA_TRY(cudaMemsetAsync(O.scatter, 0, nb, st));
@@ -342,15 +354,18 @@ mcpet_status prepare_run(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies
   if (O.spectrum) CUDA_TRY(cudaMemsetAsync(O.spectrum, 0, (size_t)sc->cfg.n_energy_bins * 4, st));
   CUDA_TRY(cudaMemsetAsync(O.psf_count, 0, 4, st));
   CUDA_TRY(cudaMemsetAsync(O.histories, 0, 8, st));
-  if (!O.coincidences) O.coincidences = sc->dev.small + 14;
   CUDA_TRY(cudaMemsetAsync(O.coincidences, 0, 8, st));
-  if (!sc->cfg.tally_material_dose) O.mat_dose = nullptr;
-  if (dose_voxels(sc->cfg) == 0) O.vox_dose = nullptr;
   if (O.mat_dose) CUDA_TRY(cudaMemsetAsync(O.mat_dose, 0, 2 * kMaxMaterials * 8, st));
   if (O.vox_dose) CUDA_TRY(cudaMemsetAsync(O.vox_dose, 0, (size_t)dose_voxels(sc->cfg) * 16, st));
-  /* the kernel only touches the spectrum when the sinogram is tallied */
-  if (!sino) P.spectrum_in_shared = 0;
   return MCPET_OK;
+}
+
+/* Parameters of one scene's run and its zeroed outputs. */
+mcpet_status prepare_run(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies& O, cudaStream_t st,
+                         TransportParams& P) {
+  mcpet_status s = prepare_params(sc, o, O, P);
+  if (s != MCPET_OK) return s;
+  return zero_outputs(sc, O, st);
 }
 
 int pick_block(const mcpet_run_opts& o) {
@@ -617,23 +632,32 @@ mcpet_status check_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   return merge_shared_tables(scenes, n, U ? *U : local);
 }
 
-/* Enqueue ONE launch of the event kernel over the lanes of all scenes.
- * outs[k] are scene k's device tallies.  Each scene keeps its own lane plan
- * (cached on the scene like a single run's), seed and RANECU stream numbers,
- * so its tallies equal those of a run of that scene alone. */
-mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts* opts, DeviceTallies* outs,
-                           cudaStream_t st, double* ms_out) {
+/* Everything one batched launch needs, built on the host: the scenes' slots
+ * (parameters, tables, tallies, first lane), the union Compton/Rayleigh
+ * tables, the launch-wide parameters and the launch shape. */
+struct BatchLaunch {
+  std::vector<SceneSlot> slots;
   SharedTables U;
-  mcpet_status cs = check_batch(scenes, n, opts, &U);
-  if (cs != MCPET_OK) return cs;
-  if (!outs) return set_error(MCPET_ERR_ARG, "null argument");
-  mcpet_run_opts def;
-  memset(&def, 0, sizeof(def));
-  const mcpet_run_opts& o = opts ? *opts : def;
-  mcpet_scene* s0 = scenes[0];
-  std::vector<SceneSlot> slots((size_t)n);
-  int max_shells = 1;
+  TransportParams P;
+  DeviceTables T;
   uint64_t total = 0;
+  bool counters = false, dose = false;
+  int grid = 1, block = 0;
+  size_t smem = 0;
+  /* device blob: slots | Compton table | Rayleigh float rows | Rayleigh byte rows */
+  size_t off_cmp = 0, off_ray = 0, off_ray8 = 0, bytes = 0;
+};
+
+/* Lane plans, tables and parameters of a batch (no stream work but the
+ * uploads of tables and plans).  outs[k] are scene k's device tallies. */
+mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts& o, const DeviceTallies* outs,
+                         BatchLaunch& L) {
+  mcpet_status cs = check_batch(scenes, n, &o, &L.U);
+  if (cs != MCPET_OK) return cs;
+  mcpet_scene* s0 = scenes[0];
+  L.slots.assign((size_t)n, SceneSlot{});
+  int max_shells = 1;
+  L.total = 0;
   for (int k = 0; k < n; ++k) {
     mcpet_scene* sc = scenes[k];
     sc->dev.run_h2d = 0;
@@ -650,79 +674,131 @@ mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_op
     const int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
     s = build_lanes(sc, o.lane_mode, tpb, hpl);
     if (s != MCPET_OK) return s;
-    SceneSlot& z = slots[(size_t)k];
+    SceneSlot& z = L.slots[(size_t)k];
     memset(&z, 0, sizeof(z));
     z.O = outs[k];
-    s = prepare_run(sc, o, z.O, st, z.P);
+    s = prepare_params(sc, o, z.O, z.P);
     if (s != MCPET_OK) return s;
     z.P.spectrum_in_shared = 0;
     z.P.palette_in_shared = 0;
     z.P.n_lanes = sc->dev.n_lanes;
     z.P.n_emitters = sc->dev.n_emitters;
     z.T = device_tables(sc);
-    z.first_lane = total;
-    total += sc->dev.n_lanes;
+    z.first_lane = L.total;
+    L.total += sc->dev.n_lanes;
     max_shells = std::max(max_shells, z.P.max_shells);
-    CUDA_TRY(cudaMemsetAsync(sc->dev.small, 0, sizeof(unsigned long long), st));  /* guard word */
   }
   CUDA_TRY(cudaSetDevice(s0->dev.device));
 
-  /* per-call device data: the slots and the union tables, released in stream order */
   const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
-  const size_t off_cmp = ((slots.size() * sizeof(SceneSlot) + 255) / 256) * 256;
-  const size_t off_ray = off_cmp + ((sizeof(ComptonTable) + 255) / 256) * 256;
-  const size_t off_ray8 = off_ray + 4 * nr * sizeof(float);
-  const size_t bytes = off_ray8 + 2 * nr;
-  std::vector<unsigned char> host(bytes, 0);
-  memcpy(host.data(), slots.data(), slots.size() * sizeof(SceneSlot));
-  memcpy(host.data() + off_cmp, &U.cmp, sizeof(ComptonTable));
-  memcpy(host.data() + off_ray, U.ray.data(), 4 * nr * sizeof(float));
-  memcpy(host.data() + off_ray8, U.ray8.data(), 2 * nr);
-  unsigned char* dbuf = nullptr;
-  CUDA_TRY(cudaMallocAsync((void**)&dbuf, bytes, st));
-  CUDA_TRY(cudaMemcpyAsync(dbuf, host.data(), bytes, cudaMemcpyHostToDevice, st));
-  for (int k = 0; k < n; ++k) scenes[k]->dev.last_h2d = scenes[k]->dev.run_h2d;
-  s0->dev.last_h2d += (long long)bytes;
+  L.off_cmp = ((L.slots.size() * sizeof(SceneSlot) + 255) / 256) * 256;
+  L.off_ray = L.off_cmp + ((sizeof(ComptonTable) + 255) / 256) * 256;
+  L.off_ray8 = L.off_ray + 4 * nr * sizeof(float);
+  L.bytes = L.off_ray8 + 2 * nr;
 
-  /* launch-wide view: lane count, work queue and guard in scene 0's words */
-  TransportParams P = slots[0].P;
-  P.n_lanes = total;
-  P.n_emitters = 0;
-  P.max_shells = max_shells;
-  DeviceTables T = slots[0].T;
-  T.emitters = nullptr;
-  T.compton = reinterpret_cast<const ComptonTable*>(dbuf + off_cmp);
-  const float* ray = reinterpret_cast<const float*>(dbuf + off_ray);
-  T.rayleigh.xco = ray;
-  T.rayleigh.pco = ray + nr;
-  T.rayleigh.aco = ray + 2 * nr;
-  T.rayleigh.bco = ray + 3 * nr;
-  T.rayleigh.itl = dbuf + off_ray8;
-  T.rayleigh.itu = dbuf + off_ray8 + nr;
+  /* launch-wide view: lane count, the union tables (pointers set once the
+   * blob is on the device) */
+  L.P = L.slots[0].P;
+  L.P.n_lanes = L.total;
+  L.P.n_emitters = 0;
+  L.P.max_shells = max_shells;
+  L.T = L.slots[0].T;
+  L.T.emitters = nullptr;
+  L.counters = o.collect_counters && outs[0].counters;
+  L.block = pick_block(o);
+  L.smem = transport_dynamic_smem(L.P, L.block, kAlgorithmEvents);
+  int bps = 0;
+  L.dose = false;
+  for (const SceneSlot& z : L.slots) L.dose = L.dose || z.O.mat_dose || z.O.vox_dose;
+  CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.block, L.smem, &bps));
+  if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", L.smem);
+  if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
+  L.grid = L.total == 0 ? 1 : s0->dev.sm_count * bps;
+  return MCPET_OK;
+}
+
+/* Host image of the batch's device blob. */
+std::vector<unsigned char> batch_blob(const BatchLaunch& L) {
+  const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
+  std::vector<unsigned char> host(L.bytes, 0);
+  memcpy(host.data(), L.slots.data(), L.slots.size() * sizeof(SceneSlot));
+  memcpy(host.data() + L.off_cmp, &L.U.cmp, sizeof(ComptonTable));
+  memcpy(host.data() + L.off_ray, L.U.ray.data(), 4 * nr * sizeof(float));
+  memcpy(host.data() + L.off_ray8, L.U.ray8.data(), 2 * nr);
+  return host;
+}
+
+/* Point the launch-wide tables at the blob on the device. */
+void bind_blob(BatchLaunch& L, unsigned char* dbuf) {
+  const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
+  L.T.compton = reinterpret_cast<const ComptonTable*>(dbuf + L.off_cmp);
+  const float* ray = reinterpret_cast<const float*>(dbuf + L.off_ray);
+  L.T.rayleigh.xco = ray;
+  L.T.rayleigh.pco = ray + nr;
+  L.T.rayleigh.aco = ray + 2 * nr;
+  L.T.rayleigh.bco = ray + 3 * nr;
+  L.T.rayleigh.itl = dbuf + L.off_ray8;
+  L.T.rayleigh.itu = dbuf + L.off_ray8 + nr;
+}
+
+/* Stream work of one batched launch: zero the scenes' outputs and the
+ * launch words (guard, lane cursor, counters), then the kernel. */
+mcpet_status enqueue_batch_launch(mcpet_scene* const* scenes, int n, BatchLaunch& L, unsigned char* dbuf,
+                                  unsigned long long* guard, unsigned long long* cursor, cudaStream_t st,
+                                  cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
+  for (int k = 0; k < n; ++k) {
+    mcpet_status s = zero_outputs(scenes[k], L.slots[(size_t)k].O, st);
+    if (s != MCPET_OK) return s;
+  }
   DeviceTallies O;
   memset(&O, 0, sizeof(O));
-  O.guard = s0->dev.small + 0;
-  O.lane_cursor = s0->dev.small + 1;
-  CUDA_TRY(cudaMemsetAsync(O.lane_cursor, 0, sizeof(unsigned long long), st));
-  const bool counters = o.collect_counters && outs[0].counters;
-  if (counters) {
-    O.counters = outs[0].counters;
+  O.guard = guard;
+  O.lane_cursor = cursor;
+  CUDA_TRY(cudaMemsetAsync(guard, 0, sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
+  if (L.counters) {
+    O.counters = L.slots[0].O.counters;
     CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
   }
-  const int block = pick_block(o);
-  const size_t smem = transport_dynamic_smem(P, block, kAlgorithmEvents);
-  int bps = 0;
-  bool dose = false;
-  for (const SceneSlot& z : slots) dose = dose || z.O.mat_dose || z.O.vox_dose;
-  CUDA_TRY(transport_batch_occupancy(counters, dose, block, smem, &bps));
-  if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
-  if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
-  const int grid = total == 0 ? 1 : s0->dev.sm_count * bps;
+  if (ev0) CUDA_TRY(cudaEventRecord(ev0, st));
+  CUDA_TRY(launch_transport_batch(L.P, L.T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, L.counters, L.dose,
+                                  L.grid, L.block, L.smem, st));
+  if (ev1) CUDA_TRY(cudaEventRecord(ev1, st));
+  return MCPET_OK;
+}
+
+/* Enqueue ONE launch of the event kernel over the lanes of all scenes.
+ * outs[k] are scene k's device tallies.  Each scene keeps its own lane plan
+ * (cached on the scene like a single run's), seed and RANECU stream numbers,
+ * so its tallies equal those of a run of that scene alone. */
+mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts* opts, DeviceTallies* outs,
+                           cudaStream_t st, double* ms_out) {
+  if (!outs) return set_error(MCPET_ERR_ARG, "null argument");
+  mcpet_run_opts def;
+  memset(&def, 0, sizeof(def));
+  const mcpet_run_opts& o = opts ? *opts : def;
+  BatchLaunch L;
+  mcpet_status s = setup_batch(scenes, n, o, outs, L);
+  if (s != MCPET_OK) return s;
+  for (int k = 0; k < n; ++k) outs[k] = L.slots[(size_t)k].O;
+  mcpet_scene* s0 = scenes[0];
+  /* per-call device data: the slots and the union tables, released in stream order */
+  const std::vector<unsigned char> host = batch_blob(L);
+  unsigned char* dbuf = nullptr;
+  CUDA_TRY(cudaMallocAsync((void**)&dbuf, L.bytes, st));
+  CUDA_TRY(cudaMemcpyAsync(dbuf, host.data(), L.bytes, cudaMemcpyHostToDevice, st));
+  for (int k = 0; k < n; ++k) scenes[k]->dev.last_h2d = scenes[k]->dev.run_h2d;
+  s0->dev.last_h2d += (long long)L.bytes;
+  bind_blob(L, dbuf);
   auto& d = s0->dev;
-  if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
-  CUDA_TRY(launch_transport_batch(P, T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, counters, dose, grid, block,
-                                  smem, st));
-  if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
+  /* the launch's guard and work queue are scene 0's words */
+  for (int k = 1; k < n; ++k) CUDA_TRY(cudaMemsetAsync(scenes[k]->dev.small, 0, sizeof(unsigned long long), st));
+  s = enqueue_batch_launch(scenes, n, L, dbuf, d.small + 0, d.small + 1, st,
+                           ms_out ? (cudaEvent_t)d.ev0 : nullptr, ms_out ? (cudaEvent_t)d.ev1 : nullptr);
+  if (s != MCPET_OK) {
+    cudaFreeAsync(dbuf, st);
+    return s;
+  }
   CUDA_TRY(cudaFreeAsync(dbuf, st));
   if (ms_out) {
     CUDA_TRY(cudaEventSynchronize((cudaEvent_t)d.ev1));
@@ -970,6 +1046,242 @@ mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, co
   if (s == MCPET_OK && device_outs[0].transport_ms) *device_outs[0].transport_ms = ms;
   return s;
 }
+
+}  // extern "C"
+
+/* A captured batched launch that regenerates its histories on every replay. */
+struct mcpet_batch_graph {
+  int device = -1;
+  std::vector<mcpet_scene*> scenes;
+  BatchLaunch L;
+  unsigned char* dbuf = nullptr;              /* slots + union tables */
+  mcpet::Emitter* plans = nullptr;            /* copies of the scenes' lane plans */
+  unsigned long long* words = nullptr;        /* guard, lane cursor, default coincidence words */
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~mcpet_batch_graph() {
+    if (device >= 0) cudaSetDevice(device);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (dbuf) cudaFree(dbuf);
+    if (plans) cudaFree(plans);
+    if (words) cudaFree(words);
+  }
+};
+
+extern "C" {
+
+mcpet_status mcpet_batch_graph_create(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                                      const mcpet_tallies* device_outs, int seed_step, mcpet_batch_graph** out) {
+  using namespace mcpet;
+  if (!out) return set_error(MCPET_ERR_ARG, "null output");
+  *out = nullptr;
+  mcpet_status cs = check_batch(scenes, n_scenes, opts, nullptr);
+  if (cs != MCPET_OK) return cs;
+  if (!device_outs) return set_error(MCPET_ERR_ARG, "null argument");
+  if (seed_step < 0) return set_error(MCPET_ERR_ARG, "seed step must be >= 0 (got %d)", seed_step);
+  mcpet_run_opts o;
+  memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  o.stream = nullptr;
+  std::unique_ptr<mcpet_batch_graph> g(new (std::nothrow) mcpet_batch_graph());
+  if (!g) return set_error(MCPET_ERR_NOMEM, "out of host memory");
+  mcpet_status s = scenes[0]->dev.device < 0 ? mcpet_scene_to_device(scenes[0], -1) : ensure_device(scenes[0]);
+  if (s != MCPET_OK) return s;
+  g->device = scenes[0]->dev.device;
+  g->scenes.assign(scenes, scenes + n_scenes);
+  CUDA_TRY(cudaMalloc((void**)&g->words, (size_t)(2 + n_scenes) * sizeof(unsigned long long)));
+  CUDA_TRY(cudaMemset(g->words, 0, (size_t)(2 + n_scenes) * sizeof(unsigned long long)));
+  std::vector<DeviceTallies> outs((size_t)n_scenes);
+  for (int k = 0; k < n_scenes; ++k) {
+    outs[(size_t)k] = tallies_from(&device_outs[k]);
+    if (!outs[(size_t)k].coincidences) outs[(size_t)k].coincidences = g->words + 2 + k;
+  }
+  BatchLaunch& L = g->L;
+  s = setup_batch(scenes, n_scenes, o, outs.data(), L);
+  if (s != MCPET_OK) return s;
+  /* own copies of the lane plans: later runs of the scenes may rebuild theirs */
+  size_t n_em = 0;
+  for (int k = 0; k < n_scenes; ++k) n_em += (size_t)scenes[k]->dev.n_emitters;
+  CUDA_TRY(cudaMalloc((void**)&g->plans, std::max<size_t>(n_em, 1) * sizeof(Emitter)));
+  size_t off = 0;
+  for (int k = 0; k < n_scenes; ++k) {
+    const auto& d = scenes[k]->dev;
+    if (d.n_emitters > 0)
+      CUDA_TRY(cudaMemcpy(g->plans + off, d.emitters, (size_t)d.n_emitters * sizeof(Emitter),
+                          cudaMemcpyDeviceToDevice));
+    L.slots[(size_t)k].T.emitters = g->plans + off;
+    off += (size_t)d.n_emitters;
+  }
+  CUDA_TRY(cudaMalloc((void**)&g->dbuf, L.bytes));
+  const std::vector<unsigned char> host = batch_blob(L);
+  CUDA_TRY(cudaMemcpy(g->dbuf, host.data(), L.bytes, cudaMemcpyHostToDevice));
+  bind_blob(L, g->dbuf);
+
+  /* capture: zero the outputs, the launch, then the seeds of the next replay */
+  cudaStream_t cap = nullptr;
+  CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    s = enqueue_batch_launch(scenes, n_scenes, L, g->dbuf, g->words + 0, g->words + 1, cap);
+    if (s == MCPET_OK) {
+      cudaError_t le = launch_advance_seeds(reinterpret_cast<SceneSlot*>(g->dbuf), n_scenes, seed_step, cap);
+      if (le != cudaSuccess) s = set_error(MCPET_ERR_CUDA, "CUDA error: %s", cudaGetErrorString(le));
+    }
+    e = cudaStreamEndCapture(cap, &g->graph);
+  }
+  cudaStreamDestroy(cap);
+  if (s != MCPET_OK) return s;
+  if (e != cudaSuccess) return set_error(MCPET_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  CUDA_TRY(cudaGraphInstantiate(&g->exec, g->graph, 0));
+  *out = g.release();
+  return MCPET_OK;
+}
+
+/* Autotuner: time candidate (histories per lane, threads per block) pairs
+ * on a sample of the workload and keep the fastest.  The sample runs every
+ * scene with its acquisition time scaled by f and the candidate's histories
+ * per lane scaled by the same f, so it has the full workload's lane count and
+ * lane order with f of its decays: per-lane work, fill and tail keep their
+ * proportions. */
+mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
+                            const mcpet_tallies* device_outs, double sample_decays, mcpet_tune_result* out) {
+  using namespace mcpet;
+  if (!out || !device_outs) return set_error(MCPET_ERR_ARG, "null argument");
+  memset(out, 0, sizeof(*out));
+  mcpet_run_opts o;
+  memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  if (n_scenes > 1) {
+    mcpet_status cs = check_batch(scenes, n_scenes, &o, nullptr);
+    if (cs != MCPET_OK) return cs;
+  } else {
+    if (n_scenes != 1 || !scenes || !scenes[0]) return set_error(MCPET_ERR_ARG, "autotune needs at least one scene");
+    mcpet_status cs = validate_opts(scenes[0], &o);
+    if (cs != MCPET_OK) return cs;
+  }
+  o.collect_counters = 0;
+  const bool balanced = o.lane_mode == MCPET_LANES_BALANCED;
+  for (int k = 0; k < n_scenes; ++k) {
+    mcpet_status s = (k > 0 && scenes[k]->dev.device < 0) ? mcpet_scene_to_device(scenes[k], scenes[0]->dev.device)
+                                                          : ensure_device(scenes[k]);
+    if (s != MCPET_OK) return s;
+  }
+  /* decays of the workload and the automatic histories per lane of its
+   * largest scene: the centre of the candidates */
+  double D = 0, d_max = -1;
+  int base = 1;
+  for (int k = 0; k < n_scenes; ++k) {
+    const mcpet_scene* sc = scenes[k];
+    double T = (double)sc->cfg.acquisition_time_ps * 1e-12, dk = 0;
+    for (float a : sc->activity)
+      if (a > 1.0e-7f) dk += (double)a * T;
+    D += dk;
+    if (dk > d_max) {
+      d_max = dk;
+      base = auto_hpl(sc);
+    }
+  }
+  std::vector<int> hpls;
+  if (balanced) {
+    const int c[5] = {std::max(1, base / 4), std::max(1, base / 2), base, 2 * base, 4 * base};
+    for (int v : c)
+      if (std::find(hpls.begin(), hpls.end(), v) == hpls.end()) hpls.push_back(v);
+  } else {
+    hpls.push_back(0);   /* reference lanes: the plan is fixed, only the block size is tuned */
+  }
+  double f = (sample_decays > 0 ? sample_decays : 2.0e8) / std::max(D, 1.0);
+  if (balanced) f = std::max(f, 1.0 / (double)hpls.front());
+  if (f > 1.0) f = 1.0;
+  out->sample_fraction = f;
+
+  std::vector<unsigned long long> acq((size_t)n_scenes);
+  for (int k = 0; k < n_scenes; ++k) {
+    acq[(size_t)k] = scenes[k]->cfg.acquisition_time_ps;
+    scenes[k]->cfg.acquisition_time_ps = (unsigned long long)llround((double)acq[(size_t)k] * f);
+    scenes[k]->dev.activity_dirty = true;
+  }
+  std::vector<DeviceTallies> outs((size_t)n_scenes);
+  cudaStream_t st = (cudaStream_t)o.stream;
+  auto time_one = [&](int hpl, int block, double* ms) -> mcpet_status {
+    mcpet_run_opts c = o;
+    c.histories_per_lane = balanced ? std::max(1, (int)llround(hpl * f)) : 0;
+    c.block_threads = block;
+    for (int k = 0; k < n_scenes; ++k) outs[(size_t)k] = tallies_from(&device_outs[k]);
+    if (n_scenes == 1) return enqueue_run(scenes[0], &c, outs[0], st, ms);
+    return enqueue_batch(scenes, n_scenes, &c, outs.data(), st, ms);
+  };
+  mcpet_status s = MCPET_OK;
+  double best = 1e300, ms = 0;
+  int best_hpl = hpls[0], best_block = transport_block_threads();
+  /* first the histories per lane at the full block, then the block size */
+  s = time_one(base, best_block, &ms);   /* warm-up: clocks, tables, first plan */
+  for (size_t i = 0; s == MCPET_OK && i < hpls.size(); ++i) {
+    s = time_one(hpls[i], transport_block_threads(), &ms);
+    ++out->candidates;
+    if (s == MCPET_OK && hpls[i] == (balanced ? base : 0)) out->auto_ms = ms;
+    if (s == MCPET_OK && ms < best) {
+      best = ms;
+      best_hpl = hpls[i];
+    }
+  }
+  const int blocks[2] = {128, 192};
+  for (int i = 0; s == MCPET_OK && i < 2; ++i) {
+    if (blocks[i] >= transport_block_threads()) continue;
+    s = time_one(best_hpl, blocks[i], &ms);
+    ++out->candidates;
+    if (s == MCPET_OK && ms < best) {
+      best = ms;
+      best_block = blocks[i];
+    }
+  }
+  for (int k = 0; k < n_scenes; ++k) {
+    scenes[k]->cfg.acquisition_time_ps = acq[(size_t)k];
+    scenes[k]->dev.activity_dirty = true;
+  }
+  if (s != MCPET_OK) return s;
+  out->histories_per_lane = balanced ? best_hpl : 0;
+  out->block_threads = best_block;
+  out->best_ms = best;
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_batch_graph_launch(mcpet_batch_graph* g, void* stream) {
+  using namespace mcpet;
+  if (!g || !g->exec) return set_error(MCPET_ERR_ARG, "null graph");
+  CUDA_TRY(cudaSetDevice(g->device));
+  CUDA_TRY(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_batch_graph_set_seeds(mcpet_batch_graph* g, const int* seeds, void* stream) {
+  using namespace mcpet;
+  if (!g || !seeds) return set_error(MCPET_ERR_ARG, "null argument");
+  const int n = (int)g->scenes.size();
+  for (int k = 0; k < n; ++k)
+    if (seeds[k] <= 0 || seeds[k] >= (int)2147483563)
+      return set_error(MCPET_ERR_ARG, "seed %d of scene %d outside [1, 2147483562]", seeds[k], k);
+  CUDA_TRY(cudaSetDevice(g->device));
+  for (int k = 0; k < n; ++k) {
+    g->L.slots[(size_t)k].P.seed = seeds[k];
+    unsigned char* dst = g->dbuf + (size_t)k * sizeof(SceneSlot) + offsetof(SceneSlot, P) +
+                         offsetof(TransportParams, seed);
+    CUDA_TRY(cudaMemcpyAsync(dst, &g->L.slots[(size_t)k].P.seed, sizeof(int), cudaMemcpyHostToDevice,
+                             (cudaStream_t)stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_batch_graph_guard_trips(mcpet_batch_graph* g, unsigned long long* trips) {
+  using namespace mcpet;
+  if (!g || !trips) return set_error(MCPET_ERR_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(g->device));
+  CUDA_TRY(cudaMemcpy(trips, g->words, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return MCPET_OK;
+}
+
+void mcpet_batch_graph_destroy(mcpet_batch_graph* g) { delete g; }
 
 mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                              mcpet_tallies* outs) {

@@ -1405,6 +1405,20 @@ cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables&
   return cudaGetLastError();
 }
 
+__global__ void advance_seeds_kernel(SceneSlot* slots, int n_slots, int step) {
+  const long long m = (long long)kM1 - 1;   /* seeds stay in [1, m1 - 1] */
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_slots; k += gridDim.x * blockDim.x) {
+    const long long s = ((long long)slots[k].P.seed - 1 + step) % m;
+    slots[k].P.seed = (int)(s < 0 ? s + m : s) + 1;
+  }
+}
+
+cudaError_t launch_advance_seeds(SceneSlot* slots, int n_slots, int step, cudaStream_t stream) {
+  const int grid = (n_slots + 127) / 128;
+  advance_seeds_kernel<<<grid > 0 ? grid : 1, 128, 0, stream>>>(slots, n_slots, step);
+  return cudaGetLastError();
+}
+
 /* Device address of the scratch array, looked up once per device with that
  * device current (the array's host-side name is only a stand-in). */
 static std::mutex g_scratch_mutex;

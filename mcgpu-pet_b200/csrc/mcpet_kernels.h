@@ -26,6 +26,10 @@ cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables&
                                    const SceneSlot* slots, int n_slots, bool counters, bool dose, int grid,
                                    int block, size_t smem, cudaStream_t stream);
 
+/* batched regeneration: advance every slot's RANECU seed by `step` within
+ * [1, m1 - 1] (the next replay of a captured batch) */
+cudaError_t launch_advance_seeds(SceneSlot* slots, int n_slots, int step, cudaStream_t stream);
+
 /* allocation-free runs: lane plan and work-queue words in a static device array */
 constexpr int kNoAllocMaxVoxels = 1 << 20;
 cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,

@@ -5,12 +5,12 @@ compute runs in the CUDA kernels of the library; there is no CPU path.
 """
 from ._abi import (ALGORITHM_AUTO, ALGORITHM_EVENTS, ALGORITHM_HISTORIES, LANES_BALANCED, LANES_REFERENCE,
                    MAX_MATERIALS, McpetError, EXPORTED, LIB_PATH, lib)
-from .scene import (PSF_DTYPE, RunOptions, RunResult, Scene, probe_compton, probe_detector, probe_rayleigh,
-                    probe_rng, probe_source, read_config)
+from .scene import (PSF_DTYPE, BatchGraph, RunOptions, RunResult, Scene, autotune, device_tallies_for,
+                    probe_compton, probe_detector, probe_rayleigh, probe_rng, probe_source, read_config)
 
 __all__ = [
     "ALGORITHM_AUTO", "ALGORITHM_EVENTS", "ALGORITHM_HISTORIES", "LANES_BALANCED", "LANES_REFERENCE", "MAX_MATERIALS", "McpetError", "EXPORTED", "LIB_PATH", "lib", "PSF_DTYPE",
-    "RunOptions", "RunResult", "Scene", "probe_compton", "probe_detector", "probe_rayleigh", "probe_rng",
+    "BatchGraph", "RunOptions", "RunResult", "Scene", "autotune", "device_tallies_for", "probe_compton", "probe_detector", "probe_rayleigh", "probe_rng",
     "probe_source", "read_config",
 ]
 

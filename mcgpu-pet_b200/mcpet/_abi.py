@@ -170,6 +170,17 @@ class GradArgs(C.Structure):
     ]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("block_threads", C.c_int),
+        ("histories_per_lane", C.c_int),
+        ("best_ms", C.c_double),
+        ("auto_ms", C.c_double),
+        ("sample_fraction", C.c_double),
+        ("candidates", C.c_int),
+    ]
+
+
 EVENT_RECORD_BYTES = 24
 
 PSF_SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_longlong, C.c_void_p)
@@ -193,6 +204,14 @@ _SIGNATURES = {
     "mcpet_run_batch_device": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_device_noalloc": (C.c_int, [P, P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_last_run_guard": (C.c_int, [P, C.POINTER(C.c_ulonglong)]),
+    "mcpet_autotune": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies), C.c_double,
+                                 C.POINTER(TuneResult)]),
+    "mcpet_batch_graph_create": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies), C.c_int,
+                                           C.POINTER(P)]),
+    "mcpet_batch_graph_launch": (C.c_int, [P, P]),
+    "mcpet_batch_graph_set_seeds": (C.c_int, [P, P, P]),
+    "mcpet_batch_graph_guard_trips": (C.c_int, [P, C.POINTER(C.c_ulonglong)]),
+    "mcpet_batch_graph_destroy": (None, [P]),
     "mcpet_write_outputs": (C.c_int, [P, C.POINTER(Tallies), C.c_char_p, C.c_int, C.c_double]),
     "mcpet_probe_rng": (C.c_int, [C.c_int, C.c_int, P, C.c_int, P, P, P]),
     "mcpet_probe_detector": (C.c_int, [P, C.c_int] + [P] * 10),

@@ -93,6 +93,115 @@ PSF_DTYPE = np.dtype(
 assert PSF_DTYPE.itemsize == _abi.PSF_RECORD_BYTES
 
 
+def _device_tallies(tallies: dict) -> _abi.Tallies:
+    """mcpet_tallies over a dict of torch CUDA tensors (see Scene.run_device)."""
+    def p(name):
+        x = tallies.get(name)
+        return None if x is None else x.data_ptr()
+
+    t = _abi.Tallies()
+    t.trues, t.scatter = p("trues"), p("scatter")
+    t.image_trues, t.image_scatter = p("image_trues"), p("image_scatter")
+    t.spectrum = p("spectrum")
+    t.psf = p("psf")
+    t.psf_capacity = 0 if tallies.get("psf") is None else tallies["psf"].numel() // _abi.PSF_RECORD_BYTES
+    t.psf_count = p("psf_count")
+    t.total_histories = p("histories")
+    t.coincidences = p("coincidences")
+    t.counters = p("counters")
+    t.material_dose = p("material_dose")
+    t.voxel_dose = p("voxel_dose")
+    return t
+
+
+def device_tallies_for(scene: "Scene", device=None, psf_capacity: int = 0) -> dict:
+    """Fresh torch CUDA tensors for one scene's device tallies."""
+    import torch
+    dev = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+    cfg, info = scene.config, scene.info
+    nb, nv, ne = int(cfg.n_bins), int(info.n_voxels), int(cfg.n_energy_bins)
+    t = {
+        "trues": torch.empty(nb, dtype=torch.int32, device=dev),
+        "scatter": torch.empty(nb, dtype=torch.int32, device=dev),
+        "image_trues": torch.empty(nv, dtype=torch.int32, device=dev),
+        "image_scatter": torch.empty(nv, dtype=torch.int32, device=dev),
+        "spectrum": torch.empty(ne, dtype=torch.int32, device=dev),
+        "psf_count": torch.zeros(1, dtype=torch.int32, device=dev),
+        "histories": torch.zeros(1, dtype=torch.int64, device=dev),
+        "coincidences": torch.zeros(1, dtype=torch.int64, device=dev),
+    }
+    if psf_capacity > 0:
+        t["psf"] = torch.empty(psf_capacity * _abi.PSF_RECORD_BYTES, dtype=torch.uint8, device=dev)
+    return t
+
+
+def autotune(scenes: list, tallies: list, opts: Optional[RunOptions] = None,
+             sample_decays: float = 2.0e8) -> tuple:
+    """Pick histories_per_lane and block_threads for these scenes
+    (mcpet_autotune): returns (RunOptions with the chosen values, dict with
+    the sample times).  ``tallies[k]`` are scene k's device tallies (as for
+    Scene.run_device); they are overwritten."""
+    import dataclasses
+    opts = opts or RunOptions(lane_mode=_abi.LANES_BALANCED)
+    arr = (_abi.Tallies * len(scenes))(*[_device_tallies(t) for t in tallies])
+    ptrs = (C.c_void_p * max(len(scenes), 1))(*[sc._h.value for sc in scenes])
+    co = opts.to_c()
+    r = _abi.TuneResult()
+    check(lib().mcpet_autotune(ptrs, len(scenes), C.byref(co), arr, float(sample_decays), C.byref(r)))
+    tuned = dataclasses.replace(opts, block_threads=r.block_threads,
+                                histories_per_lane=r.histories_per_lane or opts.histories_per_lane)
+    return tuned, {"block_threads": r.block_threads, "histories_per_lane": r.histories_per_lane,
+                   "best_ms": r.best_ms, "auto_ms": r.auto_ms, "sample_fraction": r.sample_fraction,
+                   "candidates": r.candidates}
+
+
+class BatchGraph:
+    """A batched run captured in a CUDA graph (mcpet_batch_graph_*): every
+    launch() regenerates all scenes' histories with the next seeds (seed_k +
+    r * seed_step) into ``tallies[k]`` (torch CUDA tensors, as for
+    Scene.run_device), with one graph launch and no host work."""
+
+    def __init__(self, scenes: list, tallies: list, opts: Optional[RunOptions] = None, seed_step: int = 1):
+        opts = opts or RunOptions(lane_mode=_abi.LANES_BALANCED)
+        self._scenes = list(scenes)          # the graph reads their device data
+        self._tallies = list(tallies)
+        arr = (_abi.Tallies * len(scenes))(*[_device_tallies(t) for t in tallies])
+        ptrs = (C.c_void_p * max(len(scenes), 1))(*[sc._h.value for sc in scenes])
+        co = opts.to_c()
+        h = C.c_void_p()
+        check(lib().mcpet_batch_graph_create(ptrs, len(scenes), C.byref(co), arr, int(seed_step), C.byref(h)))
+        self._h = h
+
+    def launch(self, stream=None) -> None:
+        check(lib().mcpet_batch_graph_launch(self._h, stream))
+
+    def set_seeds(self, seeds, stream=None) -> None:
+        a = (C.c_int * len(self._scenes))(*[int(x) for x in seeds])
+        check(lib().mcpet_batch_graph_set_seeds(self._h, C.cast(a, C.c_void_p), stream))
+
+    def guard_trips(self) -> int:
+        v = C.c_ulonglong(0)
+        check(lib().mcpet_batch_graph_guard_trips(self._h, C.byref(v)))
+        return int(v.value)
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            lib().mcpet_batch_graph_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def read_config(in_path: str) -> _abi.Config:
     cfg = _abi.Config()
     check(lib().mcpet_config_read(os.fsencode(in_path), C.byref(cfg)))
@@ -336,25 +445,27 @@ class Scene:
         a uint8 psf[capacity*44] and int64 counters[10]).  Returns the
         transport time in ms when ``time_it`` (this synchronises)."""
         opts = opts or RunOptions()
-
-        def p(name):
-            x = tallies.get(name)
-            return None if x is None else x.data_ptr()
-
         ms = C.c_double(0)
-        t = _abi.Tallies()
-        t.trues, t.scatter = p("trues"), p("scatter")
-        t.image_trues, t.image_scatter = p("image_trues"), p("image_scatter")
-        t.spectrum = p("spectrum")
-        t.psf = p("psf")
-        t.psf_capacity = 0 if tallies.get("psf") is None else tallies["psf"].numel() // _abi.PSF_RECORD_BYTES
-        t.psf_count = p("psf_count")
-        t.total_histories = p("histories")
-        t.coincidences = p("coincidences")
-        t.counters = p("counters")
+        t = _device_tallies(tallies)
         t.transport_ms = C.addressof(ms) if time_it else None
         co = opts.to_c()
         check(lib().mcpet_run_device(self._h, C.byref(co), C.byref(t)))
+        return float(ms.value)
+
+    @staticmethod
+    def run_batch_device(scenes: list, tallies: list, opts: Optional[RunOptions] = None,
+                         time_it: bool = False) -> float:
+        """Several scenes in one launch into device tallies
+        (mcpet_run_batch_device); ``tallies[k]`` as for run_device.  Returns
+        the launch's transport time in ms when ``time_it``."""
+        opts = opts or RunOptions()
+        ms = C.c_double(0)
+        arr = (_abi.Tallies * len(scenes))(*[_device_tallies(t) for t in tallies])
+        if time_it:
+            arr[0].transport_ms = C.addressof(ms)
+        ptrs = (C.c_void_p * max(len(scenes), 1))(*[sc._h.value for sc in scenes])
+        co = opts.to_c()
+        check(lib().mcpet_run_batch_device(ptrs, len(scenes), C.byref(co), arr))
         return float(ms.value)
 
     def guard_trips(self) -> int:

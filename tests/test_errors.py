@@ -237,3 +237,37 @@ def test_psf_stream_argument_checks(workdir):
     assert b"chunk_records" in L.mcpet_last_error()
     assert L.mcpet_run_psf_stream(psf.handle, None, 64, None, None, C.byref(t)) == ERR["arg"]
     psf.close()
+
+
+def test_batch_graph_and_autotune_argument_errors(workdir):
+    """Host-side checks of the graph and autotuner entry points (no device work)."""
+    import ctypes as C
+    L = _abi.lib()
+    h = C.c_void_p()
+    t = (_abi.Tallies * 1)()
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_batch_graph_create(None, 0, None, t, 1, C.byref(h)))
+    assert e.value.status == ERR["arg"]
+    mat, rho, act, vs = inputs.sample_phantom()
+    sc = scenes.scene_from_arrays(workdir, mat, rho, act, vs)
+    ptrs = (C.c_void_p * 1)(sc.handle)
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_batch_graph_create(ptrs, 1, None, t, -1, C.byref(h)))
+    assert e.value.status == ERR["arg"] and "seed step" in str(e.value)
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_batch_graph_create(ptrs, 1, None, None, 1, C.byref(h)))
+    assert e.value.status == ERR["arg"]
+    for fn, args in ((L.mcpet_batch_graph_launch, (None, None)), (L.mcpet_batch_graph_set_seeds, (None, None, None)),
+                     (L.mcpet_batch_graph_guard_trips, (None, None))):
+        with pytest.raises(mcpet.McpetError) as e:
+            _abi.check(fn(*args))
+        assert e.value.status == ERR["arg"]
+    L.mcpet_batch_graph_destroy(None)
+    r = _abi.TuneResult()
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_autotune(ptrs, 1, None, None, 1e6, C.byref(r)))
+    assert e.value.status == ERR["arg"]
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_autotune(ptrs, 0, None, t, 1e6, C.byref(r)))
+    assert e.value.status == ERR["arg"]
+    sc.close()
