@@ -222,9 +222,10 @@ def _ellipsoid(shape, center, radii, vs):
     z = (np.arange(nz) + 0.5) * vs[2]
     y = (np.arange(ny) + 0.5) * vs[1]
     x = (np.arange(nx) + 0.5) * vs[0]
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    return (((X - center[0]) / radii[0]) ** 2 + ((Y - center[1]) / radii[1]) ** 2 +
-            ((Z - center[2]) / radii[2]) ** 2) <= 1.0
+    X = (((x - center[0]) / radii[0]) ** 2)[None, None, :]
+    Y = (((y - center[1]) / radii[1]) ** 2)[None, :, None]
+    Z = (((z - center[2]) / radii[2]) ** 2)[:, None, None]
+    return (X + Y + Z) <= 1.0
 
 
 def head_phantom(shape=(64, 128, 128), voxel_cm=0.2, seed: int = 2024, total_bq: float = 1.0e9):
@@ -298,6 +299,85 @@ def batch_phantoms(n: int, emissions_each: float, seed: int = 3):
         mat, rho, act, vs, used = head_phantom(shape=(m, m, m), voxel_cm=vox, seed=seed * 1000 + k,
                                                total_bq=emissions_each)
         yield mat, rho, act, vs, used
+
+
+def body_phantom(shape=(400, 256, 256), voxel_cm=0.2, seed: int = 2025, total_bq: float = 5.0e9):
+    """Seeded whole-body phantom of nested ellipsoids (z is the body axis,
+    head at high z): torso of soft tissue under a fat layer, two lungs
+    (rho 0.3), a spine and a rib shell of bone (1.85), heart blood pool,
+    a hot organ (8x background), and a head with skull, grey and white matter
+    and CSF.  Activity ratios: organ 8, grey 4, white 1, heart blood 2,
+    soft/fat 1, bone 0.3, lung 0.2, CSF and air 0; scaled to total_bq.
+    Returns (material, density, activity, voxel_size, tissues) like
+    head_phantom."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    vs = (voxel_cm, voxel_cm, voxel_cm)
+    L = np.array([nx * vs[0], ny * vs[1], nz * vs[2]])
+    jit = lambda a: a * rng.uniform(0.95, 1.05)
+    labels = np.zeros(shape, np.int8)
+    names = list(TISSUES)
+
+    def paint(center, radii, name):
+        labels[_ellipsoid(shape, center, radii, vs)] = names.index(name)
+
+    cx, cy = L[0] / 2, L[1] / 2
+    # torso over the lower 72 % of the length, head above a short neck
+    zt = 0.36 * L[2]
+    rt = np.array([jit(0.42 * L[0]), jit(0.30 * L[1]), 0.36 * L[2]])
+    paint((cx, cy, zt), rt, "fat")
+    paint((cx, cy, zt), rt - [1.2, 1.2, 0.5], "soft")
+    paint((cx, cy, zt + 0.12 * L[2]), (rt[0] - 2.0, rt[1] - 2.0, 0.16 * L[2]), "bone")     # rib shell
+    paint((cx, cy, zt + 0.12 * L[2]), (rt[0] - 2.8, rt[1] - 2.8, 0.155 * L[2]), "soft")
+    for sgn in (-1, 1):                                                                 # lungs
+        paint((cx + sgn * jit(0.19 * L[0]), cy, zt + 0.14 * L[2]), (jit(0.13 * L[0]), jit(0.19 * L[1]), 0.12 * L[2]),
+              "lung")
+    paint((cx + jit(0.04 * L[0]), cy + 0.03 * L[1], zt + 0.08 * L[2]), (jit(0.07 * L[0]),) * 2 + (0.05 * L[2],),
+          "blood")                                                                      # heart
+    paint((cx - jit(0.12 * L[0]), cy, zt - 0.04 * L[2]), (jit(0.14 * L[0]), jit(0.15 * L[1]), 0.06 * L[2]),
+          "organ")                                                                      # hot organ
+    paint((cx, cy - 0.21 * L[1], zt), (0.03 * L[0], 0.035 * L[1], 0.34 * L[2]), "bone")  # spine
+    zh = 0.87 * L[2]
+    rh = np.array([jit(0.31 * L[0]), jit(0.36 * L[1]), 0.11 * L[2]])
+    paint((cx, cy, 0.75 * L[2]), (0.12 * L[0], 0.12 * L[1], 0.05 * L[2]), "soft")      # neck
+    paint((cx, cy, zh), rh, "soft")
+    paint((cx, cy, zh), rh - 0.4, "bone")
+    paint((cx, cy, zh + 0.2), rh - 1.0, "grey")
+    paint((cx, cy, zh + 0.3), rh - 1.8, "white")
+    for sgn in (-1, 1):
+        paint((cx + sgn * 1.0, cy, zh + 0.5), (0.6, 2.0, 0.9), "csf")
+    ratio = {"air": 0.0, "soft": 1.0, "grey": 4.0, "white": 1.0, "bone": 0.3, "fat": 1.0, "blood": 2.0, "csf": 0.0,
+             "lung": 0.2, "organ": 8.0}
+    mat = np.zeros(shape, np.int32)
+    rho = np.zeros(shape, np.float32)
+    act = np.zeros(shape, np.float64)
+    for li, name in enumerate(names):
+        m = labels == li
+        if not m.any():
+            continue
+        slot, _, d = TISSUES[name]
+        mat[m] = slot
+        rho[m] = d
+        act[m] = ratio[name]
+    act *= total_bq / act.sum()
+    used = [n for i, n in enumerate(names) if (labels == i).any()]
+    return mat, rho, act.astype(np.float32), vs, used
+
+
+def scanner_long_axial(max_ring_difference: int = 255, span: int = 11, n_angles: int = 384,
+                       n_radial: int = 384) -> dict:
+    """1 m axial, 39 cm radius, 256 rings x 4 mm, 768 crystals, span 11,
+    MRD 255 (12333 sinogram planes of 384 x 384 at full size)."""
+    return dict(detector_radius=-39.0, detector_height=102.4, fov_z=102.4, n_rows=256, n_crystals=768,
+                n_angles=n_angles, n_radial=n_radial, n_z_slices=511, max_ring_difference=max_ring_difference,
+                span=span)
+
+
+def bed_centers(phantom_size_cm, n_beds: int, step_cm: float):
+    """Detector centres (x, y, z) of n_beds bed positions along the body
+    axis, step_cm apart and symmetric about the phantom's centre."""
+    cx, cy, cz = (0.5 * phantom_size_cm[0], 0.5 * phantom_size_cm[1], 0.5 * phantom_size_cm[2])
+    return [(cx, cy, cz + (k - 0.5 * (n_beds - 1)) * step_cm) for k in range(n_beds)]
 
 
 def scanner_small() -> dict:
