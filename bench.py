@@ -329,6 +329,87 @@ def measure_gradient(workdir: str, emissions: float = 2.0e8) -> dict:
             "outputs": "dL/dA and dL/ds for every voxel"}
 
 
+def measure_beds(n_beds: int, workdir: str, emissions_total: float = 5.0e9) -> dict:
+    """Long-axial body workload (config C5 shapes): 256x256x400 body phantom
+    at 2 mm with 10 tissues (lungs, bone, hot organ at 8x), 1 m scanner of
+    256 rings, 384 x 384 x 12333-plane span-11 sinograms (1.82e9 bins, int32),
+    n_beds bed positions 20 cm apart sharing emissions_total decays.  The beds
+    run batched in one launch and one by one (mcpet_run_batch_device vs
+    mcpet_run_device, device-resident tallies, CUDA events); then the
+    activity and density-scale gradient of one bed's sinogram
+    log-likelihood (mcpet_grad) against a plain forward of that bed."""
+    import torch
+    import mcpet
+    from mcpet import grad as G
+    from mcpet import inputs
+    mat, rho, act, vs, used = inputs.body_phantom(seed=2025, total_bq=emissions_total / n_beds)
+    size = tuple(n * v for n, v in zip(mat.shape[::-1], vs))
+    scan = inputs.scanner_long_axial()
+    scan["detector_radius"] = 39.0
+    beds = []
+    for k, c in enumerate(inputs.bed_centers(size, n_beds, 20.0)):
+        spec = inputs.spec_for(inputs.tissue_materials(used), "unused.vox", seed=3000 + k, detector_center=c, **scan)
+        beds.append(mcpet.Scene.from_arrays(inputs.config_from_spec(spec, workdir), mat, rho, act, vs))
+    tal = [mcpet.device_tallies_for(b) for b in beds]
+    stream = torch.cuda.current_stream()
+    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED, stream=stream.cuda_stream)
+
+    def coinc():
+        return sum(int(t["coincidences"].item()) for t in tal)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    mcpet.Scene.run_batch_device(beds, tal, opts)            # warm-up: tables, plans
+    seq_ms = timed(lambda: [b.run_device(t, opts) for b, t in zip(beds, tal)])
+    seq_c = coinc()
+    bat_ms = timed(lambda: mcpet.Scene.run_batch_device(beds, tal, opts))
+    bat_c = coinc()
+    per_bed = [int(t["coincidences"].item()) for t in tal]
+    top = int(torch.nonzero(tal[0]["trues"]).max().item()) if bool(tal[0]["trues"].any()) else -1
+    guard = beds[0].guard_trips()
+    nbins = int(beds[0].config.n_bins)
+    del tal
+    torch.cuda.empty_cache()
+
+    # gradient of bed 0: measured sinogram = another seed with the organ x1.5, plus 5 % randoms
+    b0 = beds[0]
+    act_t = act.copy()
+    act_t[mat == inputs.TISSUES["organ"][0]] *= 1.5
+    b0.set_activity(act_t)
+    t = G._device_tallies(b0, torch, torch.device("cuda"))
+    b0.run_device(t, mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED, seed_override=4242))
+    y = (t["trues"] + t["scatter"]).to(torch.float32)
+    del t
+    torch.cuda.empty_cache()
+    bg = torch.full_like(y, 0.05 * float(y.sum()) / y.numel())
+    y += torch.poisson(bg)
+    b0.set_activity(act)
+    tall = G._device_tallies(b0, torch, torch.device("cuda"))
+    G.grad(b0, y, bg, opts, tallies=tall)                    # warm-up: event buffer, device activity
+    plain = timed(lambda: b0.run_device(tall, opts))
+    r = G.grad(b0, y, bg, opts, tallies=tall)
+    for b in beds:
+        b.close()
+    rate = lambda c, ms: c / (ms * 1e-3)
+    return {"workload": f"body phantom 256x256x400 @ 2 mm, 10 tissues (lung 0.3, bone 1.85, hot organ 8x), "
+                        f"{emissions_total:.0e} decays over {n_beds} bed positions 20 cm apart; scanner R=39 cm, "
+                        f"256 rings x 4 mm, 384 x 384 x 12333 span-11 sinograms ({nbins} bins, int32) per bed",
+            "unit": UNIT, "batched": {"ms": bat_ms, "value": rate(bat_c, bat_ms), "launches": 1},
+            "one_by_one": {"ms": seq_ms, "value": rate(seq_c, seq_ms), "launches": n_beds},
+            "coincidences_per_bed": per_bed, "highest_bin_bed0": top, "guard_trips": guard,
+            "gradient_bed0": {"plain_forward_ms": plain, "forward_with_records_ms": r.forward_ms,
+                              "gradient_pass_ms": r.gradient_ms,
+                              "gradient_time_over_forward": (r.forward_ms + r.gradient_ms) / plain,
+                              "events": r.events, "replay_mismatches": r.mismatches}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -346,6 +427,8 @@ def main():
                          "launch against the same runs one by one (reported under 'batch')")
     ap.add_argument("--batch-emissions", type=float, default=1.0e8, help="decays per phantom of --batch-scenes")
     ap.add_argument("--no-gradient", action="store_true", help="skip the gradient (mcpet_grad) measurement")
+    ap.add_argument("--beds", type=int, default=0,
+                    help="also measure the long-axial body workload with this many bed positions (not a bench line)")
     ap.add_argument("--block-threads", type=int, default=0, help="threads per block (0: automatic)")
     ap.add_argument("--histories-per-lane", type=int, default=0, help="balanced lanes: decays per lane (0: automatic)")
     ap.add_argument("--scanner", default="head", choices=["head", "head32"],
@@ -494,6 +577,13 @@ def main():
     if args.batch_scenes > 0 and rank == 0:
         batch = measure_batch(args.batch_scenes, tmp, args.batch_emissions)
 
+    beds = None
+    if args.beds > 0 and rank == 0:
+        scene.close()
+        del tallies
+        torch.cuda.empty_cache()
+        beds = measure_beds(args.beds, tmp)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, desc, _, _ = cpu_reference_sample(cfg, mat, rho, act, vs, args.cpu_seconds)
@@ -516,6 +606,8 @@ def main():
             line["gradient"] = gradient
         if batch is not None:
             line["batch"] = batch
+        if beds is not None:
+            line["beds"] = beds
         print(json.dumps(line))
     scene.close()
     if dist:

@@ -130,7 +130,9 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   for (int m = 0; m < kMaxMaterials; ++m)
     if (sc->material_loaded[m] && sc->compton.noscco[m] > ms) ms = sc->compton.noscco[m];
   P.max_shells = ms;
-  P.spectrum_in_shared = (c.n_energy_bins > 0 && c.n_energy_bins <= kSpectrumSharedMax) ? 1 : 0;
+  P.spectrum_in_shared =
+      (c.n_energy_bins > 0 && c.n_energy_bins <= kSpectrumSharedMax && env_int("MCPET_SPECTRUM_SHARED", 1, 0, 1)) ? 1
+                                                                                                                : 0;
   P.palette_in_shared =
       (sc->palette.size() <= 2048 && env_int("MCPET_PALETTE_SHARED", 1, 0, 1)) ? (int)sc->palette.size() : 0;
   P.e_annihilation = 510998.95f;
@@ -646,11 +648,38 @@ struct BatchLaunch {
   DeviceTables T;
   uint64_t total = 0;
   bool counters = false, dose = false;
+  int share = 0;                    /* kBatchShareScanner | kBatchSharePhantom */
   int grid = 1, block = 0;
   size_t smem = 0;
   /* device blob: slots | Compton table | Rayleigh float rows | Rayleigh byte rows */
   size_t off_cmp = 0, off_ray = 0, off_ray8 = 0, bytes = 0;
 };
+
+/* True when scene b has scene a's scanner: detector, sinogram, energy
+ * window and tally settings, and the acquisition time of the PSF records
+ * (every parameter detect_pair reads). */
+bool same_scanner(const TransportParams& a, const TransportParams& b) {
+  return a.cx == b.cx && a.cy == b.cy && a.cz == b.cz && a.radius == b.radius && a.height == b.height &&
+         a.psf_capacity == b.psf_capacity && a.tally_psf_sinogram == b.tally_psf_sinogram &&
+         a.tally_type == b.tally_type && a.background_mode == b.background_mode && a.e_resol == b.e_resol &&
+         a.e_low == b.e_low && a.e_high == b.e_high && a.fovz == b.fovz && a.nrows == b.nrows &&
+         a.ncrystals == b.ncrystals && a.nangles == b.nangles && a.nrad == b.nrad && a.nzs == b.nzs &&
+         a.ne == b.ne && a.mrd == b.mrd && a.span == b.span && a.nsinos == b.nsinos && a.nbins == b.nbins &&
+         a.sino_dry == b.sino_dry && a.e_annihilation == b.e_annihilation && a.acq_ps == b.acq_ps;
+}
+
+/* True when scene b has scene a's phantom: grid, voxel keys, palette and
+ * the Woodcock and interaction tables. */
+bool same_phantom(const mcpet_scene* a, const mcpet_scene* b) {
+  if (a == b) return true;
+  return a->nx == b->nx && a->ny == b->ny && a->nz == b->nz &&
+         memcmp(a->voxel_size, b->voxel_size, sizeof(a->voxel_size)) == 0 &&
+         memcmp(a->bbox, b->bbox, sizeof(a->bbox)) == 0 && a->dev.vox16 == b->dev.vox16 &&
+         a->voxel_key == b->voxel_key && a->palette.size() == b->palette.size() &&
+         (a->palette.empty() ||
+          memcmp(a->palette.data(), b->palette.data(), a->palette.size() * sizeof(a->palette[0])) == 0) &&
+         a->woodcock == b->woodcock && a->mfp_a == b->mfp_a && a->mfp_b == b->mfp_b && a->pmax == b->pmax;
+}
 
 /* Lane plans, tables and parameters of a batch (no stream work but the
  * uploads of tables and plans).  outs[k] are scene k's device tallies. */
@@ -714,7 +743,16 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   int bps = 0;
   L.dose = false;
   for (const SceneSlot& z : L.slots) L.dose = L.dose || z.O.mat_dose || z.O.vox_dose;
-  CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.block, L.smem, &bps));
+  L.share = 0;
+  if (!L.counters && !L.dose) {
+    bool scanner = true, phantom = true;
+    for (int k = 1; k < n; ++k) {
+      scanner = scanner && same_scanner(L.slots[0].P, L.slots[(size_t)k].P);
+      phantom = phantom && same_phantom(s0, scenes[k]);
+    }
+    L.share = (scanner ? kBatchShareScanner : 0) | (phantom ? kBatchSharePhantom : 0);
+  }
+  CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.share, L.block, L.smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", L.smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   L.grid = L.total == 0 ? 1 : s0->dev.sm_count * bps;
@@ -766,7 +804,7 @@ mcpet_status enqueue_batch_launch(mcpet_scene* const* scenes, int n, BatchLaunch
   }
   if (ev0) CUDA_TRY(cudaEventRecord(ev0, st));
   CUDA_TRY(launch_transport_batch(L.P, L.T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, L.counters, L.dose,
-                                  L.grid, L.block, L.smem, st));
+                                  L.share, L.grid, L.block, L.smem, st));
   if (ev1) CUDA_TRY(cudaEventRecord(ev1, st));
   return MCPET_OK;
 }

@@ -381,10 +381,10 @@ __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, c
  * Detector: intersection with the ideal cylinder of radius R around the axis
  * through (cx, cy) (MCGPU-PET_kernel.cu:1645-1700).  Outputs the hit point
  * relative to the detector centre and the travelled distance. */
-__device__ __forceinline__ float to_cylinder(const TransportParams& P, const float3& pos, const float3& dir,
-                                             float& xn, float& yn, float& zn) {
-  float x0 = pos.x - P.cx;
-  float y0 = pos.y - P.cy;
+__device__ __forceinline__ float to_cylinder(const TransportParams& P, const float3& centre, const float3& pos,
+                                             const float3& dir, float& xn, float& yn, float& zn) {
+  float x0 = pos.x - centre.x;
+  float y0 = pos.y - centre.y;
   float A = dir.x * dir.x + dir.y * dir.y;
   float B = 2.0f * (x0 * dir.x + y0 * dir.y);
   float C = x0 * x0 + y0 * y0 - P.radius * P.radius;
@@ -393,8 +393,12 @@ __device__ __forceinline__ float to_cylinder(const TransportParams& P, const flo
   else dist = (-B + sqrtf(B * B - 4.0f * A * C)) / (2.0f * A);
   xn = x0 + dist * dir.x;
   yn = y0 + dist * dir.y;
-  zn = (pos.z - P.cz) + dist * dir.z;
+  zn = (pos.z - centre.z) + dist * dir.z;
   return dist;
+}
+__device__ __forceinline__ float to_cylinder(const TransportParams& P, const float3& pos, const float3& dir,
+                                             float& xn, float& yn, float& zn) {
+  return to_cylinder(P, make_float3(P.cx, P.cy, P.cz), pos, dir, xn, yn, zn);
 }
 
 /* Sinogram bin of a line of response (MCGPU-PET_kernel.cu:1749-1791) from the

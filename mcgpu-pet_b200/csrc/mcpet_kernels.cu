@@ -235,20 +235,21 @@ __device__ __forceinline__ void put_psf_record(uint32_t* psf, long long k, unsig
 /* Coincidence processing of one photon pair whose two photons escaped
  * (MCGPU-PET_kernel.cu:417-432): sinogram tally (tally_Sinogram,
  * :1624-1836) and/or phase-space tally (tally_PSF_coincidences, :531-644).
- * "b" = the second photon (tracked last), "a" = the first. */
+ * "b" = the second photon (tracked last), "a" = the first.  `centre` is the
+ * detector centre (P.cx, P.cy, P.cz). */
 template <bool kCount, bool kRecord = true>
-__device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, const DeviceTallies& O,
-                                            int* spec_sh, int voxel, unsigned long long t_left,
-                                            const PhotonState& b, const PhotonState& a, LaneCounters& cnt,
-                                            unsigned long long& detected, int2 rng_emit) {
+__device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, const float3 centre,
+                                            const DeviceTallies& O, int* spec_sh, int voxel,
+                                            unsigned long long t_left, const PhotonState& b, const PhotonState& a,
+                                            LaneCounters& cnt, unsigned long long& detected, int2 rng_emit) {
   const bool want_sino = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 2);
   const bool want_psf = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 1);
   if (want_sino) {
     float xb, yb, zb, xa, ya, za;
-    to_cylinder(P, b.pos, b.dir, xb, yb, zb);
+    to_cylinder(P, centre, b.pos, b.dir, xb, yb, zb);
     float phib = atan2f(yb, xb);
     if (fabsf(zb) < 0.5f * P.height) {
-      to_cylinder(P, a.pos, a.dir, xa, ya, za);
+      to_cylinder(P, centre, a.pos, a.dir, xa, ya, za);
       float phia = atan2f(ya, xa);
       if (fabsf(za) < 0.5f * P.height) {
         long long bin = sinogram_bin(P, phib, zb, phia, za);
@@ -315,12 +316,12 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
   }
   if (want_psf) {
     float xb, yb, zb;
-    float db = to_cylinder(P, b.pos, b.dir, xb, yb, zb);
+    float db = to_cylinder(P, centre, b.pos, b.dir, xb, yb, zb);
     float travel_b = b.travel + db;
     float phib = atan2f(yb, xb);
     if (fabsf(zb) < 0.5f * P.height) {
       float xa, ya, za;
-      float da = to_cylinder(P, a.pos, a.dir, xa, ya, za);
+      float da = to_cylinder(P, centre, a.pos, a.dir, xa, ya, za);
       float travel_a = a.travel + da;
       float phia = atan2f(ya, xa);
       float g1 = blur_psf(rng);
@@ -433,7 +434,9 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       if (esc_a && esc_b) {
         bool pass = (P.tally_type == 0) || (P.tally_type == 1 && b.state == 0 && a.state == 0) ||
                     (P.tally_type == 2 && (b.state != 0 || a.state != 0));
-        if (pass) detect_pair<kCount>(rng, P, O, spec_sh, voxel, t_left, b, a, cnt, detected, rng_emit);
+        if (pass)
+          detect_pair<kCount>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel, t_left, b, a, cnt, detected,
+                              rng_emit);
       }
     }
   }
@@ -511,8 +514,14 @@ struct ColdState {
 };
 
 
+/* Batches whose scenes all have the same scanner (detector, sinogram and
+ * tally settings) or the same phantom (grid, voxels, palette, tables) read
+ * those from the launch's parameters instead of their slots. */
+constexpr int kShareScanner = kBatchShareScanner;
+constexpr int kSharePhantom = kBatchSharePhantom;
+
 template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false, bool kBatch = false, bool kRecord = false,
-          bool kDose = false>
+          bool kDose = false, int kShare = 0>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(TransportParams P, DeviceTables T,
                                                                               DeviceTallies O,
                                                                               const SceneSlot* __restrict__ slots,
@@ -590,12 +599,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   float4 rec_hi = make_float4(0.f, 0.f, 0.f, 0.f);
 
   /* photon emitted at ph.pos with ph.dir: set up its tracking */
-  auto start_photon = [&](const TransportParams& PS, const DeviceTables& TS) {
+  /* (the scenes of a batch share the energy grid: e0 and ide are P's) */
+  auto start_photon = [&](const DeviceTables& TW) {
     ph.energy = kAnnihilation;
     ph.travel = 0.0f;
     ph.state = 0;
-    index = __float2int_rd((ph.energy - PS.e0) * PS.ide);
-    float2 w = __ldg(reinterpret_cast<const float2*>(TS.woodcock) + index);
+    index = __float2int_rd((ph.energy - P.e0) * P.ide);
+    float2 w = __ldg(reinterpret_cast<const float2*>(TW.woodcock) + index);
     mfp_w = w.x + ph.energy * w.y;
     mat_old = -1;
     steps = 0;
@@ -612,7 +622,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
     const unsigned m_end = __ballot_sync(0xffffffffu, phase == kPhEnd);
     if (!(m_dec | m_step | m_cmp | m_end)) break;
     const TransportParams& PS = kBatch ? slots[scene].P : P;
-    const DeviceTables& TS = kBatch ? slots[scene].T : T;
+    /* phantom (grid, voxels, tables) and scanner (detector, sinogram) of the
+     * current lane's scene */
+    const TransportParams& PG = (kBatch && !(kShare & kSharePhantom)) ? slots[scene].P : P;
+    const DeviceTables& TG = (kBatch && !(kShare & kSharePhantom)) ? slots[scene].T : T;
+    const TransportParams& PD = (kBatch && !(kShare & kShareScanner)) ? slots[scene].P : P;
     /* phase of this round: scattering and pair bookkeeping wait until enough
      * lanes need them; Woodcock steps fill the rest */
     const int n_cmp = __popc(m_cmp), n_pair = __popc(m_end | m_dec);
@@ -649,9 +663,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
                                 kBatch ? slots[scene].O.vox_dose : O.vox_dose};
               ds(PS, e - e_before, mat0, ph.pos);
             }
-            index = __float2int_rd((e - PS.e0) * PS.ide);
+            index = __float2int_rd((e - P.e0) * P.ide);
             if (index > -1) {
-              float2 w = __ldg(reinterpret_cast<const float2*>(TS.woodcock) + index);
+              float2 w = __ldg(reinterpret_cast<const float2*>(TG.woodcock) + index);
               mfp_w = w.x + e * w.y;
               mat_old = -2;
               ph.state = (ph.state == 0) ? 1 : 3;
@@ -687,7 +701,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           emit_second(rng, background, d0, ph.dir);
           ph.pos = make_float3(cold.f(kCOx), cold.f(kCOy), cold.f(kCOz));
           which = 2;
-          start_photon(PS, TS);
+          start_photon(TG);
         } else {
           const float ea = cold.f(kCAe);
           if (escaped && ea > -0.5f) {
@@ -697,10 +711,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             a.energy = ea;
             a.travel = cold.f(kCAt);
             a.state = (int)cold.u(kCAs);
-            const bool pass = (PS.tally_type == 0) || (PS.tally_type == 1 && ph.state == 0 && a.state == 0) ||
-                              (PS.tally_type == 2 && (ph.state != 0 || a.state != 0));
+            const bool pass = (PD.tally_type == 0) || (PD.tally_type == 1 && ph.state == 0 && a.state == 0) ||
+                              (PD.tally_type == 2 && (ph.state != 0 || a.state != 0));
             if (pass)
-              detect_pair<kCount, kRecord>(rng, PS, kBatch ? slots[scene].O : O, spec_sh, (int)cold.u(kCVox),
+              detect_pair<kCount, kRecord>(rng, PD, make_float3(PD.cx, PD.cy, PD.cz), kBatch ? slots[scene].O : O,
+                                           spec_sh, (int)cold.u(kCVox),
                                            cold.t_left(), ph, a, cnt, detected,
                                            kRecord ? make_int2((int)cold.u(kCRx), (int)cold.u(kCRy))
                                                    : make_int2(0, 0));
@@ -769,7 +784,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           cold.setf(kCOx, ph.pos.x); cold.setf(kCOy, ph.pos.y); cold.setf(kCOz, ph.pos.z);
           cold.setf(kCDx, ph.dir.x); cold.setf(kCDy, ph.dir.y); cold.setf(kCDz, ph.dir.z);
           which = 1;
-          start_photon(PN, kBatch ? slots[scene].T : T);
+          start_photon((kBatch && !(kShare & kSharePhantom)) ? slots[scene].T : T);
           break;
         }
       }
@@ -783,7 +798,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           bool go = true;
           if (fresh) {
             fresh = false;
-            if (locate(PS, ph.pos.x, ph.pos.y, ph.pos.z) < 0) {
+            if (locate(PG, ph.pos.x, ph.pos.y, ph.pos.z) < 0) {
               escaped = true;
               phase = kPhEnd;
               go = false;
@@ -795,20 +810,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             ph.pos.x += step * ph.dir.x;
             ph.pos.y += step * ph.dir.y;
             ph.pos.z += step * ph.dir.z;
-            const int vox = locate(PS, ph.pos.x, ph.pos.y, ph.pos.z);
+            const int vox = locate(PG, ph.pos.x, ph.pos.y, ph.pos.z);
             if (vox < 0) {
               escaped = true;
               phase = kPhEnd;
-            } else if ((unsigned long long)vox >= (unsigned long long)PS.n_voxels || ++steps > kMaxWoodcockSteps) {
+            } else if ((unsigned long long)vox >= (unsigned long long)PG.n_voxels || ++steps > kMaxWoodcockSteps) {
               Counting<true>::add(cnt.guard, 1);
               escaped = false;
               phase = kPhEnd;
             } else {
-              const uint32_t key = TS.vox16 ? (uint32_t)__ldg(&TS.vox16[vox]) : __ldg(&TS.vox32[vox]);
-              const PaletteEntry pe = kBatch ? TS.palette[key] : pal[key];
+              const uint32_t key = TG.vox16 ? (uint32_t)__ldg(&TG.vox16[vox]) : __ldg(&TG.vox32[vox]);
+              const PaletteEntry pe = kBatch ? TG.palette[key] : pal[key];
               mat0 = pe.mat0;
               Counting<kCount>::add(cnt.steps, 1);
-              const float2* rec = reinterpret_cast<const float2*>(TS.mfp + (size_t)index * kMaxMaterials + mat0);
+              const float2* rec = reinterpret_cast<const float2*>(TG.mfp + (size_t)index * kMaxMaterials + mat0);
               if (mat0 != mat_old) {
                 const float2 ab = __ldg(rec);
                 cax = ab.x;
@@ -1375,19 +1390,34 @@ cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, co
   return cudaGetLastError();
 }
 
-cudaError_t transport_batch_occupancy(bool counters, bool dose, int block, size_t smem, int* blocks_per_sm) {
+cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int block, size_t smem,
+                                      int* blocks_per_sm) {
   if (dose)
     return counters
                ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, true, false, true>, block, smem,
                               blocks_per_sm)
                : occupancy_of(transport_events_kernel<false, kEventBlocks, false, true, false, true>, block, smem,
                               blocks_per_sm);
-  return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, true>, block, smem, blocks_per_sm)
-                  : occupancy_of(transport_events_kernel<false, kEventBlocks, false, true>, block, smem, blocks_per_sm);
+  if (counters)
+    return occupancy_of(transport_events_kernel<true, kEventBlocks, false, true>, block, smem, blocks_per_sm);
+  switch (share) {
+    case kShareScanner:
+      return occupancy_of(transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner>,
+                          block, smem, blocks_per_sm);
+    case kSharePhantom:
+      return occupancy_of(transport_events_kernel<false, kEventBlocks, false, true, false, false, kSharePhantom>,
+                          block, smem, blocks_per_sm);
+    case kShareScanner | kSharePhantom:
+      return occupancy_of(
+          transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner | kSharePhantom>, block,
+          smem, blocks_per_sm);
+    default:
+      return occupancy_of(transport_events_kernel<false, kEventBlocks, false, true>, block, smem, blocks_per_sm);
+  }
 }
 
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int grid,
+                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int grid,
                                    int block, size_t smem, cudaStream_t stream) {
   if (dose) {
     if (counters)
@@ -1398,10 +1428,26 @@ cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables&
                                                                                                           slots, n_slots);
     return cudaGetLastError();
   }
-  if (counters)
+  if (counters) {
     transport_events_kernel<true, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
-  else
-    transport_events_kernel<false, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
+    return cudaGetLastError();
+  }
+  switch (share) {
+    case kShareScanner:
+      transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner>
+          <<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
+      break;
+    case kSharePhantom:
+      transport_events_kernel<false, kEventBlocks, false, true, false, false, kSharePhantom>
+          <<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
+      break;
+    case kShareScanner | kSharePhantom:
+      transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner | kSharePhantom>
+          <<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
+      break;
+    default:
+      transport_events_kernel<false, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
+  }
   return cudaGetLastError();
 }
 

@@ -20,10 +20,17 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream);
 
-/* batched runs: several scenes in one launch of the event kernel */
-cudaError_t transport_batch_occupancy(bool counters, bool dose, int block, size_t smem, int* blocks_per_sm);
+/* batched runs: several scenes in one launch of the event kernel.  share:
+ * bit 0 = every scene has the launch's scanner (detector, sinogram, tally
+ * settings), bit 1 = every scene has the launch's phantom (grid, voxel keys,
+ * palette, tables); those are then read from P and T (non-counting,
+ * dose-free launches only) */
+constexpr int kBatchShareScanner = 1;
+constexpr int kBatchSharePhantom = 2;
+cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int block, size_t smem,
+                                      int* blocks_per_sm);
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int grid,
+                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int grid,
                                    int block, size_t smem, cudaStream_t stream);
 
 /* batched regeneration: advance every slot's RANECU seed by `step` within
