@@ -739,7 +739,7 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   L.T.emitters = nullptr;
   L.counters = o.collect_counters && outs[0].counters;
   L.block = pick_block(o);
-  L.smem = transport_dynamic_smem(L.P, L.block, kAlgorithmEvents);
+  L.smem = transport_batch_dynamic_smem(L.P, L.block);
   int bps = 0;
   L.dose = false;
   for (const SceneSlot& z : L.slots) L.dose = L.dose || z.O.mat_dose || z.O.vox_dose;

@@ -488,8 +488,11 @@ enum : int {
   kCAe, kCAt, kCAs,                              /* photon 1 energy (-10 absorbed), travel, state */
   kCInvLo, kCInvHi, kCTLo, kCTHi, kCVox,         /* lane: 1/rate (double), remaining ps (u64), voxel */
   kCRx, kCRy,                                    /* RANECU state right before the pair's emission */
+  kCHist, kCDet,                                 /* batch only: lane photons started, coincidences tallied */
+  kCPmax,                                        /* batch only: Rayleigh pmax of the pending interaction */
   kCold
 };
+constexpr int kColdSingle = kCHist;              /* fields a single-scene launch uses (the last ones need no room) */
 
 struct ColdState {
   uint32_t* base;
@@ -574,6 +577,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   __syncthreads();
 
   LaneCounters cnt = {};
+  /* photons started and coincidences tallied: per thread, added to the
+   * run's totals at the end; in a batch per lane, in the shared per-thread
+   * state (kCHist, kCDet), added to the lane's scene's totals when the lane
+   * ends */
   unsigned long long histories = 0, detected = 0;
   const bool background = P.background_mode != 0;
   int scene = 0;            /* scene of the current lane (kBatch) */
@@ -596,9 +603,23 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   ph.state = 0;
   int index = 0, mat_old = -1, mat0 = 0, steps = 0;
   float mfp_w = 0.f, cax = 0.f, cbx = 0.f;
-  float4 rec_hi = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 rec_hi = make_float4(0.f, 0.f, 0.f, 0.f);   /* Rayleigh part of the last interaction record */
 
   /* photon emitted at ph.pos with ph.dir: set up its tracking */
+  /* batch: totals of the lane that just ended go to its scene's */
+  if (kBatch) {
+    cold.u(kCHist) = 0;
+    cold.u(kCDet) = 0;
+  }
+  auto flush_lane = [&]() {
+    if (!kBatch) return;
+    const unsigned long long h = cold.u(kCHist), c = cold.u(kCDet);
+    if (h) atomicAdd(slots[scene].O.histories, h);
+    if (c && slots[scene].O.coincidences) atomicAdd(slots[scene].O.coincidences, c);
+    cold.u(kCHist) = 0;
+    cold.u(kCDet) = 0;
+  };
+
   /* (the scenes of a batch share the energy grid: e0 and ide are P's) */
   auto start_photon = [&](const DeviceTables& TW) {
     ph.energy = kAnnihilation;
@@ -646,7 +667,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
         if (is_compton) {
           ok = sample_compton(rng, e, mat0, cmp, rn, costh, s0_ann);
         } else {
-          ok = sample_rayleigh(rng, e, mat0, rec_hi.z, T.rayleigh, costh);
+          ok = sample_rayleigh(rng, e, mat0, kBatch ? cold.f(kCPmax) : rec_hi.z, T.rayleigh, costh);
         }
         if (!ok) {
           Counting<true>::add(cnt.guard, 1);
@@ -713,12 +734,16 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             a.state = (int)cold.u(kCAs);
             const bool pass = (PD.tally_type == 0) || (PD.tally_type == 1 && ph.state == 0 && a.state == 0) ||
                               (PD.tally_type == 2 && (ph.state != 0 || a.state != 0));
-            if (pass)
+            if (pass) {
+              unsigned long long det = 0;
               detect_pair<kCount, kRecord>(rng, PD, make_float3(PD.cx, PD.cy, PD.cz), kBatch ? slots[scene].O : O,
                                            spec_sh, (int)cold.u(kCVox),
-                                           cold.t_left(), ph, a, cnt, detected,
+                                           cold.t_left(), ph, a, cnt, det,
                                            kRecord ? make_int2((int)cold.u(kCRx), (int)cold.u(kCRy))
                                                    : make_int2(0, 0));
+              if (kBatch) cold.u(kCDet) += (uint32_t)det;
+              else detected += det;
+            }
           }
           phase = kPhDecay;
         }
@@ -727,13 +752,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
       if (phase == kPhDecay) {
         for (;;) {
           if (!lane_live) {
-            if (kBatch && (histories | detected)) {
-              /* per-scene totals of the lane that just ended */
-              if (histories) atomicAdd(slots[scene].O.histories, histories);
-              if (detected && slots[scene].O.coincidences) atomicAdd(slots[scene].O.coincidences, detected);
-              histories = 0;
-              detected = 0;
-            }
+            flush_lane();
             const uint64_t lane = claim_lane(O.lane_cursor);
             if (lane >= n_lanes) {
               phase = kPhDone;
@@ -773,7 +792,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             continue;
           }
           cold.set_t_left(t_left - dt_ps);
-          histories += 2;
+          if (kBatch) cold.u(kCHist) += 2;
+          else histories += 2;
           cold.set_inv_rate(inv_act * exp(dt * PN.inv_mean_life));
           const int voxel = (int)cold.u(kCVox);
           if (kRecord) {
@@ -848,6 +868,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
                   if (randno < prob) {
                     phase = kPhCompton;
                     is_compton = false;
+                    /* a batch keeps pmax in shared memory (fewer live registers) */
+                    if (kBatch) cold.setf(kCPmax, rec_hi.z);
                   } else {
                     index = -11;
                     escaped = false;
@@ -870,8 +892,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   }
 
   if (kBatch) {
-    if (histories) atomicAdd(slots[scene].O.histories, histories);
-    if (detected && slots[scene].O.coincidences) atomicAdd(slots[scene].O.coincidences, detected);
+    flush_lane();
   } else {
     atomicAdd(O.histories, histories);
     if (detected) atomicAdd(O.coincidences, detected);
@@ -1313,8 +1334,12 @@ size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm
   if (P.spectrum_in_shared) s += ((size_t)P.ne * 4 + 15) / 16 * 16;
   if (P.palette_in_shared) s += ((size_t)P.palette_in_shared * sizeof(PaletteEntry) + 15) / 16 * 16;
   s += (size_t)(P.max_shells > 0 ? P.max_shells : 1) * block * sizeof(float);
-  if (algorithm != kAlgorithmHistories) s += (size_t)kCold * block * sizeof(uint32_t);
+  if (algorithm != kAlgorithmHistories) s += (size_t)kColdSingle * block * sizeof(uint32_t);
   return s;
+}
+
+size_t transport_batch_dynamic_smem(const TransportParams& P, int block) {
+  return transport_dynamic_smem(P, block, kAlgorithmEvents) + (size_t)(kCold - kColdSingle) * block * sizeof(uint32_t);
 }
 
 int transport_block_threads() { return kBlock; }

@@ -25,6 +25,7 @@ cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, co
  * settings), bit 1 = every scene has the launch's phantom (grid, voxel keys,
  * palette, tables); those are then read from P and T (non-counting,
  * dose-free launches only) */
+size_t transport_batch_dynamic_smem(const TransportParams& P, int block);
 constexpr int kBatchShareScanner = 1;
 constexpr int kBatchSharePhantom = 2;
 cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int block, size_t smem,
