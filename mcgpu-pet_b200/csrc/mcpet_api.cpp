@@ -140,6 +140,7 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 16, 1, 32);
   P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 32, 1, 32);
   P.step_keep = env_int("MCPET_STEP_KEEP", 2, 1, 8);
+  P.quorum_rayleigh = env_int("MCPET_QUORUM_RAYLEIGH", 2, 1, 32);
 }
 
 mcpet_status upload_tables(mcpet_scene* sc) {

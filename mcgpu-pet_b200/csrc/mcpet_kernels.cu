@@ -659,8 +659,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
 
     if (sel == 0) {
       /* ---- real scattering: Compton (MCGPU-PET_kernel.cu:351-373) or
-       * Rayleigh (:375-387), then the common direction update */
-      if (phase == kPhCompton) {
+       * Rayleigh (:375-387), then the common direction update.  Rayleigh
+       * lanes (GRAa) join a round with Compton lanes only when at least
+       * quorum_rayleigh of them wait, so that most rounds run one sampler */
+      const unsigned m_ray = __ballot_sync(0xffffffffu, phase == kPhCompton && !is_compton);
+      const bool ray_now = (m_cmp == m_ray) || (__popc(m_ray) >= P.quorum_rayleigh);
+      if (phase == kPhCompton && (is_compton || ray_now)) {
         double costh = 0.0;
         bool ok;
         float e = ph.energy;

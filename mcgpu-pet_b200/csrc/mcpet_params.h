@@ -96,6 +96,7 @@ struct TransportParams {
   int step_keep;          /* Woodcock batches continue while step_keep/8 of the stepping lanes step */
   int sino_dry;           /* 1: detector draws as usual but no sinogram, image, spectrum writes */
   int dose_roi[6];        /* voxel dose ROI x0,x1,y0,y1,z0,z1 (0-based, clamped); x1 < 0: off */
+  int quorum_rayleigh;    /* event loop: Rayleigh lanes needed to join a round with Compton lanes */
 };
 
 /* Device pointers of one scene (all read-only during transport). */

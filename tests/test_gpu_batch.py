@@ -136,3 +136,36 @@ def test_batch_rejects_invalid(tmp_path):
         _abi.check(_abi.lib().mcpet_run_batch_device(ptrs, 0, None, t))
     head.close()
     other.close()
+
+
+needs_ref_prog = pytest.mark.skipif(not __import__("refbind").available("libref_prog.so"),
+                                    reason="reference CUDA build missing")
+
+
+@needs_ref_prog
+@pytest.mark.gpu
+def test_batched_many_phantom_workload_replays_reference_runs(tmp_path, capsys):
+    """The first four phantoms of the many-phantom workload (uneven cubes at
+    2-4 mm, 1e8 decays each, 32-ring scanner), batched with the reference's
+    lane layout, replay the reference's CUDA runs of the same input files one
+    phantom at a time (its only way to run them)."""
+    import refbind
+    from test_gpu_transport import assert_replay
+    ins = []
+    for k, (mat, rho, act, vs, used) in enumerate(inputs.batch_phantoms(4, 1.0e8)):
+        ins.append(scenes.write_case(str(tmp_path), f"many{k}", mat, rho, act, vs, tissues=HEAD_TISSUES,
+                                     seed=1000 + k, **inputs.scanner_batch()))
+    sc = [mcpet.Scene.load(p) for p in ins]
+    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_REFERENCE)
+    batch = mcpet.Scene.run_batch(sc, opts)
+    ref_ms = []
+    for k, (p, s, r) in enumerate(zip(ins, sc, batch)):
+        cfg, info = s.config, s.info
+        ref = refbind.RefProg().run(p, int(cfg.n_bins), int(info.n_voxels), cfg.n_energy_bins, cwd=str(tmp_path))
+        assert_replay(cfg, r, ref)
+        ref_ms.append(ref["kernel_ms"])
+    with capsys.disabled():
+        print(f"\nreference kernels {[round(x, 1) for x in ref_ms]} ms (sum {sum(ref_ms):.1f}); batched "
+              f"{batch[0].transport_ms:.1f} ms; coincidences {[r.detected for r in batch]}")
+    for s in sc:
+        s.close()
