@@ -753,6 +753,15 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
     }
     L.share = (scanner ? kBatchShareScanner : 0) | (phantom ? kBatchSharePhantom : 0);
   }
+  /* a shared phantom's palette is staged in shared memory, as in a single run */
+  if (L.share & kBatchSharePhantom) {
+    TransportParams one;
+    fill_params(s0, one);
+    if (one.palette_in_shared) {
+      L.P.palette_in_shared = one.palette_in_shared;
+      L.smem = transport_batch_dynamic_smem(L.P, L.block);
+    }
+  }
   CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.share, L.block, L.smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", L.smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;

@@ -72,11 +72,11 @@ __device__ __forceinline__ uint32_t mulmod_pm(uint32_t a, uint32_t b, uint32_t c
   return q >= m ? q - m : q;
 }
 
-/* Start state of RANECU stream `stream` for the run seed: the reference
+/* Start state of RANECU stream `stream` for a seed: the reference
  * jumps each thread (stream+1)*555555*256 draws ahead
  * (init_PRNG, MCGPU-PET_kernel.cu:925-978).  a^((s+1)C) = prod over the set
  * bits of (s+1) of (a^C)^(2^k), with the 32 powers precomputed on the host. */
-__device__ __forceinline__ Rng rng_stream(const TransportParams& P, uint64_t stream) {
+__device__ __forceinline__ Rng rng_stream(const TransportParams& P, int seed, uint64_t stream) {
   uint64_t e = stream + 1;
   uint32_t y1 = 1, y2 = 1;
 #pragma unroll 4
@@ -87,9 +87,12 @@ __device__ __forceinline__ Rng rng_stream(const TransportParams& P, uint64_t str
     }
   }
   Rng r;
-  r.x = (int)mulmod_pm((uint32_t)P.seed % kM1, y1, 85u, kM1);
-  r.y = (int)mulmod_pm((uint32_t)P.seed % kM2, y2, 249u, kM2);
+  r.x = (int)mulmod_pm((uint32_t)seed % kM1, y1, 85u, kM1);
+  r.y = (int)mulmod_pm((uint32_t)seed % kM2, y2, 249u, kM2);
   return r;
+}
+__device__ __forceinline__ Rng rng_stream(const TransportParams& P, uint64_t stream) {
+  return rng_stream(P, P.seed, stream);
 }
 
 /* ------------------------------------------------------------------------

@@ -578,9 +578,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
 
   LaneCounters cnt = {};
   /* photons started and coincidences tallied: per thread, added to the
-   * run's totals at the end; in a batch per lane, in the shared per-thread
-   * state (kCHist, kCDet), added to the lane's scene's totals when the lane
-   * ends */
+   * run's totals at the end; in a batch per thread and scene, in the shared
+   * per-thread state (kCHist, kCDet), added to the scene's totals when the
+   * thread moves to another scene and at the end */
   unsigned long long histories = 0, detected = 0;
   const bool background = P.background_mode != 0;
   int scene = 0;            /* scene of the current lane (kBatch) */
@@ -606,7 +606,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   float4 rec_hi = make_float4(0.f, 0.f, 0.f, 0.f);   /* Rayleigh part of the last interaction record */
 
   /* photon emitted at ph.pos with ph.dir: set up its tracking */
-  /* batch: totals of the lane that just ended go to its scene's */
+  /* batch: the thread's totals for its current scene, added to that
+   * scene's when the thread moves to another scene and at the end */
   if (kBatch) {
     cold.u(kCHist) = 0;
     cold.u(kCDet) = 0;
@@ -756,7 +757,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
       if (phase == kPhDecay) {
         for (;;) {
           if (!lane_live) {
-            flush_lane();
             const uint64_t lane = claim_lane(O.lane_cursor);
             if (lane >= n_lanes) {
               phase = kPhDone;
@@ -772,6 +772,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
                 if (__ldg(&slots[mid].first_lane) <= lane) lo = mid;
                 else hi = mid - 1;
               }
+              if (lo != scene) flush_lane();   /* totals go to a scene when the thread leaves it */
               scene = lo;
               local = lane - __ldg(&slots[scene].first_lane);
               plan = slots[scene].T.emitters;
@@ -779,7 +780,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             }
             const Emitter* em = plan + find_emitter(plan, plan_n, local);
             const TransportParams& PN = kBatch ? slots[scene].P : P;
-            rng = rng_stream(PN, __ldg(&em->stream_base) + (local - __ldg(&em->first_lane)));
+            /* the jump tables are the same for every scene: the launch's */
+            rng = rng_stream(P, PN.seed, __ldg(&em->stream_base) + (local - __ldg(&em->first_lane)));
             cold.set_inv_rate(__ldg(&em->inv_rate));
             cold.set_t_left(PN.acq_ps);
             cold.u(kCVox) = __ldg(&em->voxel);
@@ -796,7 +798,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             continue;
           }
           cold.set_t_left(t_left - dt_ps);
-          if (kBatch) cold.u(kCHist) += 2;
+          if (kBatch) {
+            cold.u(kCHist) += 2;
+            if (cold.u(kCHist) >= 0x80000000u) flush_lane();   /* keep the 32-bit word from wrapping */
+          }
           else histories += 2;
           cold.set_inv_rate(inv_act * exp(dt * PN.inv_mean_life));
           const int voxel = (int)cold.u(kCVox);
@@ -844,7 +849,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
               phase = kPhEnd;
             } else {
               const uint32_t key = TG.vox16 ? (uint32_t)__ldg(&TG.vox16[vox]) : __ldg(&TG.vox32[vox]);
-              const PaletteEntry pe = kBatch ? TG.palette[key] : pal[key];
+              const PaletteEntry pe = (kBatch && !(kShare & kSharePhantom)) ? TG.palette[key] : pal[key];
               mat0 = pe.mat0;
               Counting<kCount>::add(cnt.steps, 1);
               const float2* rec = reinterpret_cast<const float2*>(TG.mfp + (size_t)index * kMaxMaterials + mat0);
