@@ -238,7 +238,10 @@ mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
  * use the same material files in the same slots (the Compton and Rayleigh
  * tables are shared by the launch) and sit on one device (scenes not yet on
  * a device are placed on scene 0's).  opts applies to every scene
- * (algorithm 0 or 2 only).  outs[k] receives scene k's tallies as in
+ * (algorithm 0 or 2 only); with automatic histories per lane (<= 0) the
+ * batch sizes its balanced lanes from all scenes' decays, which share the
+ * GPU, so a scene's tallies equal mcpet_run of it alone with that explicit
+ * value.  outs[k] receives scene k's tallies as in
  * mcpet_run; counters, when requested, are totals of the launch and go to
  * outs[0], and mcpet_last_run_guard(scenes[0]) reports the launch's guard
  * trips.  Blocking. */
@@ -309,8 +312,8 @@ mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, co
  * decays (f = sample_decays / total decays, raised so that every candidate
  * keeps at least one decay per lane; sample_decays <= 0 means 2e8).
  * Candidates: 1/4, 1/2, 1, 2 and 4 times the automatic histories per lane of
- * the largest scene at the full block, then smaller blocks at the best of
- * those.  Runs go through mcpet_run_device (one scene) or
+ * the workload (for several scenes, the batch's: from all their decays) at
+ * the full block, then smaller blocks at the best of those.  Runs go through mcpet_run_device (one scene) or
  * mcpet_run_batch_device (several) with opts and overwrite device_outs.  The
  * scenes' own settings are restored.  The result goes into
  * opts->histories_per_lane / block_threads of later runs; with reference

@@ -293,6 +293,7 @@ mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
   d.run_h2d += (long long)(em.size() * sizeof(Emitter));
   d.n_emitters = (int)em.size();
   d.n_lanes = lanes;
+  d.max_lane_decays = em.empty() ? 0.0 : (double)sc->cfg.acquisition_time_ps * 1e-12 / em[0].inv_rate;
   d.plan_key = key;
   d.activity_dirty = false;
   return MCPET_OK;
@@ -308,16 +309,27 @@ mcpet_status ensure_device(mcpet_scene* sc) {
  * Fewer, longer lanes amortise the per-lane start (stream jump, emitter
  * search); on the 1e9-decay head workload the kernel time falls from 774 ms
  * at 16 lanes per thread to 748 ms at 3 and stays flat down to 1. */
-int auto_hpl(const mcpet_scene* sc) {
-  double T = (double)sc->cfg.acquisition_time_ps * 1e-12, D = 0;
-  for (float a : sc->activity)
-    if (a > 1.0e-7f) D += (double)a * T;
-  double threads = (double)std::max(sc->dev.sm_count, 1) * 2048.0;
+/* Sum of the emitting voxels' activity, cached until the activity changes. */
+double emitting_activity(const mcpet_scene* sc) {
+  if (sc->emitting_activity < 0) {
+    double A = 0;
+    for (float a : sc->activity)
+      if (a > 1.0e-7f) A += (double)a;
+    const_cast<mcpet_scene*>(sc)->emitting_activity = A;
+  }
+  return sc->emitting_activity;
+}
+
+int auto_hpl_of(const std::vector<const mcpet_scene*>& scenes) {
+  double D = 0;
+  for (const mcpet_scene* sc : scenes) D += emitting_activity(sc) * ((double)sc->cfg.acquisition_time_ps * 1e-12);
+  double threads = (double)std::max(scenes[0]->dev.sm_count, 1) * 2048.0;
   double h = D / (threads * 3.0);
   if (h < 1) h = 1;
   if (h > 4096) h = 4096;
   return (int)h;
 }
+int auto_hpl(const mcpet_scene* sc) { return auto_hpl_of(std::vector<const mcpet_scene*>(1, sc)); }
 
 mcpet_status validate_opts(const mcpet_scene* sc, const mcpet_run_opts* opts) {
   int seed = (opts && opts->seed_override != 0) ? opts->seed_override : sc->cfg.seed;
@@ -643,7 +655,10 @@ mcpet_status check_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
  * (parameters, tables, tallies, first lane), the union Compton/Rayleigh
  * tables, the launch-wide parameters and the launch shape. */
 struct BatchLaunch {
-  std::vector<SceneSlot> slots;
+  std::vector<SceneSlot> slots;     /* launch order: longest lanes first */
+  std::vector<int> scene_of;        /* scene index of each slot */
+  std::vector<int> slot_of;         /* slot of each scene */
+  unsigned long long* counter_words = nullptr;  /* scene 0's counters (launch totals) */
   SharedTables U;
   TransportParams P;
   DeviceTables T;
@@ -692,6 +707,9 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   L.slots.assign((size_t)n, SceneSlot{});
   int max_shells = 1;
   L.total = 0;
+  /* automatic lanes of a batch: sized from all scenes' decays, which share
+   * the GPU (the scenes run alone with this value give the same tallies) */
+  int batch_hpl = o.histories_per_lane;
   for (int k = 0; k < n; ++k) {
     mcpet_scene* sc = scenes[k];
     sc->dev.run_h2d = 0;
@@ -704,9 +722,9 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
                        s0->dev.device);
     s = upload_tables(sc);
     if (s != MCPET_OK) return s;
+    if (batch_hpl <= 0) batch_hpl = auto_hpl_of(std::vector<const mcpet_scene*>(scenes, scenes + n));
     const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
-    const int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
-    s = build_lanes(sc, o.lane_mode, tpb, hpl);
+    s = build_lanes(sc, o.lane_mode, tpb, batch_hpl);
     if (s != MCPET_OK) return s;
     SceneSlot& z = L.slots[(size_t)k];
     memset(&z, 0, sizeof(z));
@@ -718,11 +736,30 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
     z.P.n_lanes = sc->dev.n_lanes;
     z.P.n_emitters = sc->dev.n_emitters;
     z.T = device_tables(sc);
-    z.first_lane = L.total;
-    L.total += sc->dev.n_lanes;
     max_shells = std::max(max_shells, z.P.max_shells);
   }
   CUDA_TRY(cudaSetDevice(s0->dev.device));
+  /* launch order: scenes with longer lanes first, so that no scene's longest
+   * lanes start near the end of the launch (each scene's plan is itself
+   * ordered longest first); results do not depend on the order */
+  L.scene_of.resize((size_t)n);
+  for (int k = 0; k < n; ++k) L.scene_of[(size_t)k] = k;
+  std::stable_sort(L.scene_of.begin(), L.scene_of.end(), [&](int a, int b) {
+    return scenes[a]->dev.max_lane_decays > scenes[b]->dev.max_lane_decays;
+  });
+  {
+    std::vector<SceneSlot> by_scene;
+    by_scene.swap(L.slots);
+    L.slots.resize((size_t)n);
+    L.slot_of.resize((size_t)n);
+    for (int j = 0; j < n; ++j) {
+      const int k = L.scene_of[(size_t)j];
+      L.slots[(size_t)j] = by_scene[(size_t)k];
+      L.slot_of[(size_t)k] = j;
+      L.slots[(size_t)j].first_lane = L.total;
+      L.total += scenes[k]->dev.n_lanes;
+    }
+  }
 
   const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
   L.off_cmp = ((L.slots.size() * sizeof(SceneSlot) + 255) / 256) * 256;
@@ -739,6 +776,7 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   L.T = L.slots[0].T;
   L.T.emitters = nullptr;
   L.counters = o.collect_counters && outs[0].counters;
+  L.counter_words = L.counters ? outs[0].counters : nullptr;
   L.block = pick_block(o);
   L.smem = transport_batch_dynamic_smem(L.P, L.block);
   int bps = 0;
@@ -799,7 +837,7 @@ mcpet_status enqueue_batch_launch(mcpet_scene* const* scenes, int n, BatchLaunch
                                   unsigned long long* guard, unsigned long long* cursor, cudaStream_t st,
                                   cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
   for (int k = 0; k < n; ++k) {
-    mcpet_status s = zero_outputs(scenes[k], L.slots[(size_t)k].O, st);
+    mcpet_status s = zero_outputs(scenes[k], L.slots[(size_t)L.slot_of[(size_t)k]].O, st);
     if (s != MCPET_OK) return s;
   }
   DeviceTallies O;
@@ -809,7 +847,7 @@ mcpet_status enqueue_batch_launch(mcpet_scene* const* scenes, int n, BatchLaunch
   CUDA_TRY(cudaMemsetAsync(guard, 0, sizeof(unsigned long long), st));
   CUDA_TRY(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
   if (L.counters) {
-    O.counters = L.slots[0].O.counters;
+    O.counters = L.counter_words;
     CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
   }
   if (ev0) CUDA_TRY(cudaEventRecord(ev0, st));
@@ -832,7 +870,7 @@ mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_op
   BatchLaunch L;
   mcpet_status s = setup_batch(scenes, n, o, outs, L);
   if (s != MCPET_OK) return s;
-  for (int k = 0; k < n; ++k) outs[k] = L.slots[(size_t)k].O;
+  for (int k = 0; k < n; ++k) outs[k] = L.slots[(size_t)L.slot_of[(size_t)k]].O;
   mcpet_scene* s0 = scenes[0];
   /* per-call device data: the slots and the union tables, released in stream order */
   const std::vector<unsigned char> host = batch_blob(L);
@@ -936,6 +974,7 @@ mcpet_status mcpet_scene_set_activity(mcpet_scene* sc, const float* activity) {
   if (!sc || !activity) return set_error(MCPET_ERR_ARG, "null argument");
   std::copy(activity, activity + sc->activity.size(), sc->activity.begin());
   sc->dev.activity_dirty = true;
+  sc->emitting_activity = -1;
   return MCPET_OK;
 }
 
@@ -1162,7 +1201,7 @@ mcpet_status mcpet_batch_graph_create(mcpet_scene* const* scenes, int n_scenes, 
     if (d.n_emitters > 0)
       CUDA_TRY(cudaMemcpy(g->plans + off, d.emitters, (size_t)d.n_emitters * sizeof(Emitter),
                           cudaMemcpyDeviceToDevice));
-    L.slots[(size_t)k].T.emitters = g->plans + off;
+    L.slots[(size_t)L.slot_of[(size_t)k]].T.emitters = g->plans + off;
     off += (size_t)d.n_emitters;
   }
   CUDA_TRY(cudaMalloc((void**)&g->dbuf, L.bytes));
@@ -1219,21 +1258,12 @@ mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpe
                                                           : ensure_device(scenes[k]);
     if (s != MCPET_OK) return s;
   }
-  /* decays of the workload and the automatic histories per lane of its
-   * largest scene: the centre of the candidates */
-  double D = 0, d_max = -1;
-  int base = 1;
-  for (int k = 0; k < n_scenes; ++k) {
-    const mcpet_scene* sc = scenes[k];
-    double T = (double)sc->cfg.acquisition_time_ps * 1e-12, dk = 0;
-    for (float a : sc->activity)
-      if (a > 1.0e-7f) dk += (double)a * T;
-    D += dk;
-    if (dk > d_max) {
-      d_max = dk;
-      base = auto_hpl(sc);
-    }
-  }
+  /* decays of the workload and its automatic histories per lane (the
+   * batch's, from all scenes' decays): the centre of the candidates */
+  double D = 0;
+  for (int k = 0; k < n_scenes; ++k)
+    D += emitting_activity(scenes[k]) * ((double)scenes[k]->cfg.acquisition_time_ps * 1e-12);
+  const int base = auto_hpl_of(std::vector<const mcpet_scene*>(scenes, scenes + n_scenes));
   std::vector<int> hpls;
   if (balanced) {
     const int c[5] = {std::max(1, base / 4), std::max(1, base / 2), base, 2 * base, 4 * base};
@@ -1315,10 +1345,10 @@ mcpet_status mcpet_batch_graph_set_seeds(mcpet_batch_graph* g, const int* seeds,
       return set_error(MCPET_ERR_ARG, "seed %d of scene %d outside [1, 2147483562]", seeds[k], k);
   CUDA_TRY(cudaSetDevice(g->device));
   for (int k = 0; k < n; ++k) {
-    g->L.slots[(size_t)k].P.seed = seeds[k];
-    unsigned char* dst = g->dbuf + (size_t)k * sizeof(SceneSlot) + offsetof(SceneSlot, P) +
-                         offsetof(TransportParams, seed);
-    CUDA_TRY(cudaMemcpyAsync(dst, &g->L.slots[(size_t)k].P.seed, sizeof(int), cudaMemcpyHostToDevice,
+    const size_t j = (size_t)g->L.slot_of[(size_t)k];
+    g->L.slots[j].P.seed = seeds[k];
+    unsigned char* dst = g->dbuf + j * sizeof(SceneSlot) + offsetof(SceneSlot, P) + offsetof(TransportParams, seed);
+    CUDA_TRY(cudaMemcpyAsync(dst, &g->L.slots[j].P.seed, sizeof(int), cudaMemcpyHostToDevice,
                              (cudaStream_t)stream));
   }
   CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
@@ -1416,9 +1446,7 @@ mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_talli
     long long cap = g->event_capacity;
     if (!ev) {
       if (d.event_cap <= 0) {
-        double expect = 0, T = (double)sc->cfg.acquisition_time_ps * 1e-12;
-        for (float a : sc->activity)
-          if (a > 1.0e-7f) expect += (double)a * T;
+        const double expect = emitting_activity(sc) * ((double)sc->cfg.acquisition_time_ps * 1e-12);
         long long want = (long long)std::min(std::max(expect * 0.15, 1.0e6), 2.0e9);
         CUDA_TRY(dmalloc(&d.events, (size_t)want * sizeof(EventRecord)));
         d.event_cap = want;

@@ -18,6 +18,7 @@ struct mcpet_scene {
   std::vector<int32_t> mat0;      /* 0-based material per voxel */
   std::vector<float> rho;         /* density per voxel, scaled by the density factor */
   std::vector<float> activity;    /* Bq per voxel */
+  double emitting_activity = -1;  /* sum of the emitting voxels' activity (Bq); < 0: not yet summed */
   float density_max[mcpet::kMaxMaterials];
   float density_nominal[mcpet::kMaxMaterials];
 
@@ -55,6 +56,7 @@ struct mcpet_scene {
     size_t emitters_cap = 0;
     int n_emitters = 0;
     uint64_t n_lanes = 0;
+    double max_lane_decays = 0;   /* expected decays of the plan's longest lane */
     std::string plan_key;
     /* run scratch owned by the scene (host-buffer runs) */
     int* trues = nullptr;
