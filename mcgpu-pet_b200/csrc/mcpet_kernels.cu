@@ -12,6 +12,7 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <mutex>
@@ -1353,11 +1354,24 @@ size_t transport_batch_dynamic_smem(const TransportParams& P, int block) {
 
 int transport_block_threads() { return kBlock; }
 
+/* Shared-memory carveout in percent (MCPET_CARVEOUT, for measurements), or
+ * -1 for the largest shared-memory configuration. */
+static int carveout_percent() {
+  static const int v = [] {
+    const char* e = getenv("MCPET_CARVEOUT");
+    if (!e || !*e) return -1;
+    const int p = atoi(e);
+    return (p >= 0 && p <= 100) ? p : -1;
+  }();
+  return v;
+}
+
 template <typename K>
 static cudaError_t occupancy_smem_attr(K kernel, size_t smem) {
   /* prefer shared memory over L1 so that the block count is set by registers */
+  const int pct = carveout_percent();
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       (int)cudaSharedmemCarveoutMaxShared);
+                                       pct >= 0 ? pct : (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   /* static + dynamic above 48 KB needs the opt-in, so always state the size */
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
