@@ -8,9 +8,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
 #include <memory>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mcpet.h"
@@ -230,42 +232,90 @@ DeviceTables device_tables(const mcpet_scene* sc) {
 /* Lane plan: emitters (voxels with activity > 1e-7 Bq, the reference's
  * threshold at MCGPU-PET_kernel.cu:232) with their lane counts and RANECU
  * streams, ordered by decreasing expected decays per lane. */
+/* Lane plan on the host: one emitter per voxel with activity, ordered by
+ * decreasing work per lane (ascending 1/rate per lane; ties in voxel order).
+ * The voxels are split over host threads, each building and stably sorting
+ * 16-byte keys of its range; neighbouring ranges are merged stably, which
+ * gives exactly the order of one stable sort over all voxels. */
 mcpet_status plan_host(const mcpet_scene* sc, int mode, int tpb, int hpl, std::vector<Emitter>& em,
                        uint64_t& n_lanes) {
+  struct Key {
+    double inv_rate;
+    uint32_t voxel;
+    uint32_t n_lanes;
+  };
+  const auto by_rate = [](const Key& x, const Key& y) { return x.inv_rate < y.inv_rate; };
   const size_t nv = sc->activity.size();
   const double T = (double)sc->cfg.acquisition_time_ps * 1e-12;
-  em.clear();
-  em.reserve(1024);
-  for (size_t v = 0; v < nv; ++v) {
-    float a = sc->activity[v];
-    if (!(a > 1.0e-7f)) continue;
-    Emitter e;
-    e.voxel = (uint32_t)v;
-    if (mode == MCPET_LANES_REFERENCE) {
-      e.n_lanes = (uint32_t)tpb;
-      e.stream_base = (uint64_t)v * (uint64_t)tpb;
-      e.inv_rate = (tpb / (double)a);
-    } else {
-      double expect = (double)a * T;
-      double L = ceil(expect / (double)hpl);
-      if (L < 1) L = 1;
-      if (L > 1.0e8) L = 1.0e8;
-      e.n_lanes = (uint32_t)L;
-      e.stream_base = 0;
-      e.inv_rate = (double)e.n_lanes / (double)a;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int parts = (int)std::max<size_t>(1, std::min<size_t>({(size_t)hw, 16, nv / 65536}));
+  std::vector<std::vector<Key>> part((size_t)parts);
+  auto build = [&](int t) {
+    const size_t v0 = nv * (size_t)t / (size_t)parts, v1 = nv * (size_t)(t + 1) / (size_t)parts;
+    std::vector<Key>& out = part[(size_t)t];
+    for (size_t v = v0; v < v1; ++v) {
+      const float a = sc->activity[v];
+      if (!(a > 1.0e-7f)) continue;
+      Key e;
+      e.voxel = (uint32_t)v;
+      if (mode == MCPET_LANES_REFERENCE) {
+        e.n_lanes = (uint32_t)tpb;
+        e.inv_rate = (tpb / (double)a);
+      } else {
+        const double expect = (double)a * T;
+        double L = ceil(expect / (double)hpl);
+        if (L < 1) L = 1;
+        if (L > 1.0e8) L = 1.0e8;
+        e.n_lanes = (uint32_t)L;
+        e.inv_rate = (double)e.n_lanes / (double)a;
+      }
+      out.push_back(e);
     }
-    e.first_lane = 0;
-    em.push_back(e);
+    std::stable_sort(out.begin(), out.end(), by_rate);
+  };
+  /* fn(ids[0]) here, the others on host threads (here too when a thread
+   * cannot be started) */
+  auto run = [](const std::vector<int>& ids, const std::function<void(int)>& fn) {
+    std::vector<std::thread> th;
+    size_t started = 1;
+    try {
+      for (; started < ids.size(); ++started) th.emplace_back(fn, ids[started]);
+    } catch (...) {
+    }
+    fn(ids[0]);
+    for (size_t i = started; i < ids.size(); ++i) fn(ids[i]);
+    for (auto& x : th) x.join();
+  };
+  {
+    std::vector<int> ids((size_t)parts);
+    std::iota(ids.begin(), ids.end(), 0);
+    run(ids, build);
   }
-  std::stable_sort(em.begin(), em.end(), [](const Emitter& x, const Emitter& y) { return x.inv_rate < y.inv_rate; });
-  uint64_t lanes = 0;
-  for (auto& e : em) {
+  for (int w = 1; w < parts; w *= 2) {
+    auto merge = [&](int t) {
+      std::vector<Key> m(part[(size_t)t].size() + part[(size_t)(t + w)].size());
+      std::merge(part[(size_t)t].begin(), part[(size_t)t].end(), part[(size_t)(t + w)].begin(),
+                 part[(size_t)(t + w)].end(), m.begin(), by_rate);
+      part[(size_t)t].swap(m);
+      std::vector<Key>().swap(part[(size_t)(t + w)]);
+    };
+    std::vector<int> ids;
+    for (int t = 0; t + w < parts; t += 2 * w) ids.push_back(t);
+    run(ids, merge);
+  }
+  const std::vector<Key>& keys = part[0];
+  em.assign(keys.size(), Emitter{});
+  uint64_t lanes = 0, max_stream = 0;
+  for (size_t i = 0; i < keys.size(); ++i) {
+    Emitter& e = em[i];
+    e.inv_rate = keys[i].inv_rate;
+    e.voxel = keys[i].voxel;
+    e.n_lanes = keys[i].n_lanes;
     e.first_lane = lanes;
-    if (mode != MCPET_LANES_REFERENCE) e.stream_base = lanes;
+    e.stream_base = (mode == MCPET_LANES_REFERENCE) ? (uint64_t)e.voxel * (uint64_t)tpb : lanes;
     lanes += e.n_lanes;
+    max_stream = std::max<uint64_t>(max_stream, e.stream_base + e.n_lanes);
   }
-  uint64_t max_stream = 0;
-  for (auto& e : em) max_stream = std::max<uint64_t>(max_stream, e.stream_base + e.n_lanes);
   if (max_stream >= (1ull << 31))
     return set_error(MCPET_ERR_LIMIT, "lane plan needs %llu RANECU streams (limit 2^31)",
                      (unsigned long long)max_stream);
