@@ -303,6 +303,25 @@ mcpet_status mcpet_grad(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_ta
 mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                                     mcpet_tallies* device_outs);
 
+/* ---- asynchronous host-buffer runs --------------------------------------
+ *
+ * mcpet_run without the wait: the plan upload, zeroing and transport are
+ * enqueued on opts->stream and the downloads into out's host buffers on a
+ * stream of the scene's own, and the call returns before any of it has run.
+ * The scene alternates between two sets of device tallies, so one run's
+ * downloads overlap the next run's transport (two runs of a scene in flight
+ * at most; the third waits in stream order for the first's downloads).
+ * out's scalar pointers (total_histories, coincidences, psf_count,
+ * counters) are written when the downloads finish; out and its buffers must
+ * stay valid until then (use pinned host buffers for copies that overlap).
+ * No PSF or dose tallies, no transport_ms.  Runs of a scene are ordered on
+ * one stream.  mcpet_run_wait blocks until every download of the scene has
+ * finished and reports guard trips of those runs as MCPET_ERR_DEVICE.
+ * Replaces the reference's blocking launch, synchronisation and downloads
+ * (MCGPU-PET.cu:483-535) for callers that run many acquisitions. */
+mcpet_status mcpet_run_async(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_tallies* out);
+mcpet_status mcpet_run_wait(mcpet_scene* scene);
+
 /* ---- autotuner ----------------------------------------------------------
  *
  * Picks histories_per_lane (balanced lanes) and block_threads for a workload

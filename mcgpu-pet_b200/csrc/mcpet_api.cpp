@@ -323,7 +323,10 @@ mcpet_status plan_host(const mcpet_scene* sc, int mode, int tpb, int hpl, std::v
   return MCPET_OK;
 }
 
-mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
+/* Lane plan of the scene for these options, rebuilt when the activity or the
+ * options changed.  The upload is ordered on st after the work already
+ * there (a run still reading the old plan on st finishes first). */
+mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl, cudaStream_t st) {
   auto& d = sc->dev;
   char key[128];
   snprintf(key, sizeof(key), "%d/%d/%d", mode, tpb, hpl);
@@ -339,7 +342,9 @@ mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl) {
     CUDA_TRY(dmalloc(&d.emitters, cap * sizeof(Emitter)));
     d.emitters_cap = cap;
   }
-  if (!em.empty()) CUDA_TRY(cudaMemcpy(d.emitters, em.data(), em.size() * sizeof(Emitter), cudaMemcpyHostToDevice));
+  /* from pageable memory the copy is staged before the call returns */
+  if (!em.empty())
+    CUDA_TRY(cudaMemcpyAsync(d.emitters, em.data(), em.size() * sizeof(Emitter), cudaMemcpyHostToDevice, st));
   d.run_h2d += (long long)(em.size() * sizeof(Emitter));
   d.n_emitters = (int)em.size();
   d.n_lanes = lanes;
@@ -462,7 +467,7 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   const mcpet_run_opts& o = opts ? *opts : def;
   int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
   int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
-  s = build_lanes(sc, o.lane_mode, tpb, hpl);
+  s = build_lanes(sc, o.lane_mode, tpb, hpl, st);
   if (s != MCPET_OK) return s;
 
   TransportParams P;
@@ -556,6 +561,21 @@ mcpet_status ensure_run_buffers(mcpet_scene* sc, bool want_psf) {
 mcpet_scene::~mcpet_scene() {
   if (dev.device >= 0) {
     cudaSetDevice(dev.device);
+    if (dev.copy_stream) {
+      cudaStreamSynchronize((cudaStream_t)dev.copy_stream);   /* outstanding asynchronous downloads */
+      cudaStreamDestroy((cudaStream_t)dev.copy_stream);
+    }
+    for (int k = 0; k < 2; ++k) {
+      if (dev.ran[k]) cudaEventDestroy((cudaEvent_t)dev.ran[k]);
+      if (dev.copied[k]) cudaEventDestroy((cudaEvent_t)dev.copied[k]);
+    }
+    if (dev.async_host) cudaFreeHost(dev.async_host);
+    dfree(dev.async_words);
+    dfree(dev.trues_b);
+    dfree(dev.scatter_b);
+    dfree(dev.img_t_b);
+    dfree(dev.img_s_b);
+    dfree(dev.spectrum_b);
     dfree(dev.vox);
     dfree(dev.palette);
     dfree(dev.woodcock);
@@ -750,7 +770,7 @@ bool same_phantom(const mcpet_scene* a, const mcpet_scene* b) {
 /* Lane plans, tables and parameters of a batch (no stream work but the
  * uploads of tables and plans).  outs[k] are scene k's device tallies. */
 mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts& o, const DeviceTallies* outs,
-                         BatchLaunch& L) {
+                         BatchLaunch& L, cudaStream_t st) {
   mcpet_status cs = check_batch(scenes, n, &o, &L.U);
   if (cs != MCPET_OK) return cs;
   mcpet_scene* s0 = scenes[0];
@@ -774,7 +794,7 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
     if (s != MCPET_OK) return s;
     if (batch_hpl <= 0) batch_hpl = auto_hpl_of(std::vector<const mcpet_scene*>(scenes, scenes + n));
     const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
-    s = build_lanes(sc, o.lane_mode, tpb, batch_hpl);
+    s = build_lanes(sc, o.lane_mode, tpb, batch_hpl, st);
     if (s != MCPET_OK) return s;
     SceneSlot& z = L.slots[(size_t)k];
     memset(&z, 0, sizeof(z));
@@ -918,7 +938,7 @@ mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_op
   memset(&def, 0, sizeof(def));
   const mcpet_run_opts& o = opts ? *opts : def;
   BatchLaunch L;
-  mcpet_status s = setup_batch(scenes, n, o, outs, L);
+  mcpet_status s = setup_batch(scenes, n, o, outs, L, st);
   if (s != MCPET_OK) return s;
   for (int k = 0; k < n; ++k) outs[k] = L.slots[(size_t)L.slot_of[(size_t)k]].O;
   mcpet_scene* s0 = scenes[0];
@@ -1174,6 +1194,158 @@ mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallie
   return download_run(sc, opts, out, want_psf, ms, st);
 }
 
+}  // extern "C"
+
+namespace {
+
+/* Second set of tallies, word snapshots, download stream and events of the
+ * asynchronous runs (allocated on first use). */
+mcpet_status ensure_async(mcpet_scene* sc) {
+  auto& d = sc->dev;
+  const long long nb = sc->cfg.n_bins, nv = (long long)sc->mat0.size();
+  const int ne = sc->cfg.n_energy_bins;
+  if (d.nbins_b != nb) {
+    dfree(d.trues_b);
+    dfree(d.scatter_b);
+    CUDA_TRY(dmalloc(&d.trues_b, (size_t)nb * 4));
+    CUDA_TRY(dmalloc(&d.scatter_b, (size_t)nb * 4));
+    d.nbins_b = nb;
+  }
+  if (d.nvox_b != nv) {
+    dfree(d.img_t_b);
+    dfree(d.img_s_b);
+    CUDA_TRY(dmalloc(&d.img_t_b, (size_t)nv * 4));
+    CUDA_TRY(dmalloc(&d.img_s_b, (size_t)nv * 4));
+    d.nvox_b = nv;
+  }
+  if (d.ne_b != ne) {
+    dfree(d.spectrum_b);
+    CUDA_TRY(dmalloc(&d.spectrum_b, (size_t)std::max(ne, 1) * 4));
+    d.ne_b = ne;
+  }
+  if (!d.async_words) CUDA_TRY(dmalloc(&d.async_words, 2 * 16 * sizeof(unsigned long long)));
+  if (!d.async_host) {
+    CUDA_TRY(cudaMallocHost((void**)&d.async_host, 2 * 16 * sizeof(unsigned long long)));
+    memset(d.async_host, 0, 2 * 16 * sizeof(unsigned long long));
+  }
+  if (!d.copy_stream) {
+    cudaStream_t cs = nullptr;
+    CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    d.copy_stream = cs;
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (!d.ran[k]) {
+      cudaEvent_t e = nullptr;
+      CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      d.ran[k] = e;
+    }
+    if (!d.copied[k]) {
+      cudaEvent_t e = nullptr;
+      CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      d.copied[k] = e;
+    }
+  }
+  return MCPET_OK;
+}
+
+/* Host function at the end of an asynchronous download: the run's scalars
+ * from the pinned snapshot into the caller's variables. */
+void CUDART_CB finish_async(void* p) {
+  const auto* a = static_cast<const mcpet_scene::Device::AsyncOut*>(p);
+  const unsigned long long* w = a->words;
+  if (a->psf_count) *a->psf_count = (int32_t)(w[3] & 0xffffffffull);
+  if (a->total_histories) *a->total_histories = w[2];
+  if (a->coincidences) *a->coincidences = w[14];
+  if (a->counters) {
+    memset(a->counters, 0, sizeof(mcpet_counters));
+    if (a->counters_on) memcpy(a->counters, w + 4, 10 * 8);
+    a->counters->guard_trips = w[0];
+  }
+  if (w[0]) __atomic_fetch_add(a->guard_sum, w[0], __ATOMIC_RELAXED);
+}
+
+}  // namespace
+
+extern "C" {
+
+mcpet_status mcpet_run_async(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out) {
+  if (!sc || !out) return set_error(MCPET_ERR_ARG, "null argument");
+  if (out->psf || out->material_dose || out->voxel_dose)
+    return set_error(MCPET_ERR_ARG, "asynchronous runs download no PSF or dose tallies (use mcpet_run)");
+  mcpet_status s = validate_opts(sc, opts);
+  if (s != MCPET_OK) return s;
+  s = ensure_device(sc);
+  if (s != MCPET_OK) return s;
+  s = upload_tables(sc);
+  if (s != MCPET_OK) return s;
+  s = ensure_run_buffers(sc, false);
+  if (s != MCPET_OK) return s;
+  s = ensure_async(sc);
+  if (s != MCPET_OK) return s;
+  auto& d = sc->dev;
+  const int k = d.async_next;
+  cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
+  cudaStream_t cs = (cudaStream_t)d.copy_stream;
+  /* set k is free again once its previous download finished */
+  if (d.copied_pending[k]) CUDA_TRY(cudaStreamWaitEvent(st, (cudaEvent_t)d.copied[k], 0));
+  DeviceTallies O;
+  memset(&O, 0, sizeof(O));
+  O.trues = k ? d.trues_b : d.trues;
+  O.scatter = k ? d.scatter_b : d.scatter;
+  O.image_trues = k ? d.img_t_b : d.img_t;
+  O.image_scatter = k ? d.img_s_b : d.img_s;
+  O.spectrum = k ? d.spectrum_b : d.spectrum;
+  O.histories = d.small + 2;
+  O.psf_count = (int*)(d.small + 3);
+  O.coincidences = d.small + 14;
+  O.counters = (opts && opts->collect_counters) ? d.small + 4 : nullptr;
+  s = enqueue_run(sc, opts, O, st, nullptr);
+  if (s != MCPET_OK) return s;
+  /* the run words are reused by the next run: snapshot them in stream order */
+  unsigned long long* words = d.async_words + 16 * k;
+  CUDA_TRY(cudaMemcpyAsync(words, d.small, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ran[k], st));
+  /* downloads on the scene's copy stream, overlapping the next run */
+  CUDA_TRY(cudaStreamWaitEvent(cs, (cudaEvent_t)d.ran[k], 0));
+  const size_t nb = (size_t)sc->cfg.n_bins * 4, nv = sc->mat0.size() * 4;
+  if (out->trues) CUDA_TRY(cudaMemcpyAsync(out->trues, O.trues, nb, cudaMemcpyDeviceToHost, cs));
+  if (out->scatter) CUDA_TRY(cudaMemcpyAsync(out->scatter, O.scatter, nb, cudaMemcpyDeviceToHost, cs));
+  if (out->image_trues) CUDA_TRY(cudaMemcpyAsync(out->image_trues, O.image_trues, nv, cudaMemcpyDeviceToHost, cs));
+  if (out->image_scatter)
+    CUDA_TRY(cudaMemcpyAsync(out->image_scatter, O.image_scatter, nv, cudaMemcpyDeviceToHost, cs));
+  if (out->spectrum)
+    CUDA_TRY(cudaMemcpyAsync(out->spectrum, O.spectrum, (size_t)sc->cfg.n_energy_bins * 4, cudaMemcpyDeviceToHost,
+                             cs));
+  unsigned long long* host_words = d.async_host + 16 * k;
+  CUDA_TRY(cudaMemcpyAsync(host_words, words, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, cs));
+  auto& a = d.async_out[k];
+  a.words = host_words;
+  a.psf_count = out->psf_count;
+  a.total_histories = out->total_histories;
+  a.coincidences = out->coincidences;
+  a.counters = out->counters;
+  a.counters_on = opts && opts->collect_counters;
+  a.guard_sum = &d.async_guard;
+  CUDA_TRY(cudaLaunchHostFunc(cs, finish_async, &a));
+  CUDA_TRY(cudaEventRecord((cudaEvent_t)d.copied[k], cs));
+  d.copied_pending[k] = true;
+  d.async_next = k ^ 1;
+  return MCPET_OK;
+}
+
+mcpet_status mcpet_run_wait(mcpet_scene* sc) {
+  if (!sc) return set_error(MCPET_ERR_ARG, "null argument");
+  auto& d = sc->dev;
+  if (!d.copy_stream) return MCPET_OK;
+  CUDA_TRY(cudaSetDevice(d.device));
+  CUDA_TRY(cudaStreamSynchronize((cudaStream_t)d.copy_stream));
+  d.copied_pending[0] = d.copied_pending[1] = false;
+  const unsigned long long g = __atomic_exchange_n(&d.async_guard, 0ull, __ATOMIC_RELAXED);
+  d.last_guard = g;
+  if (g != 0) return set_error(MCPET_ERR_DEVICE, "%llu device guard(s) fired (loop cap or out-of-range index)", g);
+  return MCPET_OK;
+}
+
 mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                                     mcpet_tallies* device_outs) {
   mcpet_status cs = check_batch(scenes, n_scenes, opts, nullptr);
@@ -1239,7 +1411,7 @@ mcpet_status mcpet_batch_graph_create(mcpet_scene* const* scenes, int n_scenes, 
     if (!outs[(size_t)k].coincidences) outs[(size_t)k].coincidences = g->words + 2 + k;
   }
   BatchLaunch& L = g->L;
-  s = setup_batch(scenes, n_scenes, o, outs.data(), L);
+  s = setup_batch(scenes, n_scenes, o, outs.data(), L, nullptr);
   if (s != MCPET_OK) return s;
   /* own copies of the lane plans: later runs of the scenes may rebuild theirs */
   size_t n_em = 0;
@@ -1583,10 +1755,10 @@ mcpet_status mcpet_run_psf_stream(mcpet_scene* sc, const mcpet_run_opts* opts, l
   const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
   const int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
   sc->dev.run_h2d = 0;
-  s = build_lanes(sc, o.lane_mode, tpb, hpl);
+  cudaStream_t st = (cudaStream_t)o.stream;
+  s = build_lanes(sc, o.lane_mode, tpb, hpl, st);
   if (s != MCPET_OK) return s;
   auto& d = sc->dev;
-  cudaStream_t st = (cudaStream_t)o.stream;
 
   DeviceTallies O;
   memset(&O, 0, sizeof(O));

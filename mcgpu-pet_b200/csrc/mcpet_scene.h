@@ -81,6 +81,32 @@ struct mcpet_scene {
     float* activity = nullptr;
     unsigned long long* gwords = nullptr;  /* 0 replayed, 1 mismatches, 2 log-likelihood (double) */
     unsigned long long last_guard = 0;
+    /* asynchronous host-buffer runs (mcpet_run_async): a second set of
+     * tallies, snapshots of the run words, a download stream and events */
+    int* trues_b = nullptr;
+    int* scatter_b = nullptr;
+    int* img_t_b = nullptr;
+    int* img_s_b = nullptr;
+    int* spectrum_b = nullptr;
+    long long nbins_b = -1, nvox_b = -1;
+    int ne_b = -1;
+    unsigned long long* async_words = nullptr;  /* device [2][16] */
+    unsigned long long* async_host = nullptr;   /* pinned host [2][16] */
+    void* copy_stream = nullptr;
+    void* ran[2] = {nullptr, nullptr};          /* transport of set k done */
+    void* copied[2] = {nullptr, nullptr};       /* download of set k done */
+    bool copied_pending[2] = {false, false};
+    int async_next = 0;
+    struct AsyncOut {
+      const unsigned long long* words;          /* pinned snapshot of this set's run words */
+      int32_t* psf_count;
+      unsigned long long* total_histories;
+      unsigned long long* coincidences;
+      mcpet_counters* counters;
+      bool counters_on;
+      unsigned long long* guard_sum;            /* guard trips of finished asynchronous runs */
+    } async_out[2];
+    unsigned long long async_guard = 0;
     long long run_h2d = 0;        /* host->device bytes of the run in progress */
     long long last_h2d = 0;       /* ... and of the last completed run */
   } dev;

@@ -434,6 +434,37 @@ class Scene:
         return {"coincidences": int(det.value), "total_histories": int(hist.value), "transport_ms": ms.value,
                 "psf_count": psf_count.value}
 
+    def run_async(self, host: dict, opts: Optional[RunOptions] = None) -> dict:
+        """mcpet_run_async into caller-provided host buffers (pinned torch CPU
+        tensors for overlapping copies): trues, scatter, image_trues,
+        image_scatter, spectrum.  Returns a dict of ctypes scalars
+        (coincidences, total_histories, psf_count) that hold the results once
+        wait() returned; keep it and the buffers alive until then."""
+        opts = opts or RunOptions()
+
+        def p(name):
+            x = host.get(name)
+            if x is None:
+                return None
+            return x.data_ptr() if hasattr(x, "data_ptr") else _ptr(x)
+
+        res = {"coincidences": C.c_ulonglong(0), "total_histories": C.c_ulonglong(0), "psf_count": C.c_int32(0),
+               "tallies": _abi.Tallies()}
+        t = res["tallies"]
+        t.trues, t.scatter = p("trues"), p("scatter")
+        t.image_trues, t.image_scatter = p("image_trues"), p("image_scatter")
+        t.spectrum = p("spectrum")
+        t.psf_count = C.addressof(res["psf_count"])
+        t.total_histories = C.addressof(res["total_histories"])
+        t.coincidences = C.addressof(res["coincidences"])
+        co = opts.to_c()
+        check(lib().mcpet_run_async(self._h, C.byref(co), C.byref(t)))
+        return res
+
+    def wait(self) -> None:
+        """mcpet_run_wait: block until the scene's asynchronous runs are done."""
+        check(lib().mcpet_run_wait(self._h))
+
     def last_upload_bytes(self) -> int:
         return int(self.info.last_h2d_bytes)
 

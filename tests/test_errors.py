@@ -271,3 +271,25 @@ def test_batch_graph_and_autotune_argument_errors(workdir):
         _abi.check(L.mcpet_autotune(ptrs, 0, None, t, 1e6, C.byref(r)))
     assert e.value.status == ERR["arg"]
     sc.close()
+
+
+def test_async_run_argument_errors(workdir):
+    """Host-side checks of the asynchronous entry points (no device work)."""
+    import ctypes as C
+    L = _abi.lib()
+    t = _abi.Tallies()
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_run_async(None, None, C.byref(t)))
+    assert e.value.status == ERR["arg"]
+    mat, rho, act, vs = inputs.sample_phantom()
+    sc = scenes.scene_from_arrays(workdir, mat, rho, act, vs)
+    psf = np.zeros(44, np.uint8)
+    t.psf = psf.ctypes.data
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_run_async(sc.handle, None, C.byref(t)))
+    assert e.value.status == ERR["arg"] and "PSF" in str(e.value)
+    with pytest.raises(mcpet.McpetError) as e:
+        _abi.check(L.mcpet_run_wait(None))
+    assert e.value.status == ERR["arg"]
+    _abi.check(L.mcpet_run_wait(sc.handle))      # nothing in flight
+    sc.close()

@@ -235,3 +235,35 @@ def test_outputs_written_in_reference_formats(workdir):
     raw = np.fromfile(os.path.join(out_dir, cfg.psf_file.decode() + ".raw"), dtype=mcpet.PSF_DTYPE)
     assert len(raw) == min(r.psf_count, 50000)
     assert open(os.path.join(out_dir, cfg.psf_file.decode())).read().count("\n") > min(r.psf_count, 5000)
+
+
+def test_async_runs_equal_blocking_runs(workdir):
+    """mcpet_run_async: three runs in flight on one stream with the activity
+    changed between them (the plan upload is ordered after the run still
+    reading the old plan) give the blocking runs' results."""
+    torch = pytest.importorskip("torch")
+    mat, rho, act, vs, used = inputs.head_phantom(shape=(24, 48, 48), voxel_cm=0.5, seed=3, total_bq=4e5)
+    inp = scenes.write_case(workdir, "async", mat, rho, act, vs, tissues=used, seed=2024,
+                            **inputs.scanner_batch())
+    act2 = (act * np.linspace(0.5, 1.5, act.size, dtype=np.float32).reshape(act.shape)).astype(np.float32)
+    plan = [(act, 11), (act2, 12), (act, 13)]
+    with mcpet.Scene.load(inp) as sc:
+        cfg, info = sc.config, sc.info
+        want = []
+        for a, seed in plan:
+            sc.set_activity(a)
+            want.append(sc.run(mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED, seed_override=seed)))
+        bufs, res = [], []
+        for a, seed in plan:
+            b = {k: torch.zeros(n, dtype=torch.int32).pin_memory() for k, n in
+                 (("trues", int(cfg.n_bins)), ("scatter", int(cfg.n_bins)), ("image_trues", int(info.n_voxels)),
+                  ("image_scatter", int(info.n_voxels)), ("spectrum", cfg.n_energy_bins))}
+            sc.set_activity(a)
+            res.append(sc.run_async(b, mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED, seed_override=seed)))
+            bufs.append(b)
+        sc.wait()
+        for k, (w, b, r) in enumerate(zip(want, bufs, res)):
+            for key in ("trues", "scatter", "image_trues", "image_scatter", "spectrum"):
+                np.testing.assert_array_equal(b[key].numpy(), getattr(w, key), err_msg=f"run {k}: {key}")
+            assert r["coincidences"].value == w.detected and r["total_histories"].value == w.total_histories
+        assert want[0].detected != want[1].detected
