@@ -303,6 +303,20 @@ mcpet_status mcpet_grad(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_ta
 mcpet_status mcpet_run_batch_device(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                                     mcpet_tallies* device_outs);
 
+/* Lane plan of a run with these settings, as built on the host (no device
+ * work): per emitting voxel, in launch order (decreasing work per lane,
+ * ties in voxel order), its voxel, lanes, first lane, first RANECU stream
+ * and lanes/activity.  The reference launches one block of
+ * threads_per_block lanes per voxel (MCGPU-PET.cu:456-458); lane_mode 0
+ * reproduces those lanes.  histories_per_lane <= 0: the automatic value.
+ * Any output pointer may be NULL.  With capacity below the emitter count
+ * only *n_emitters (and *total_lanes) are set and MCPET_ERR_LIMIT is
+ * returned. */
+mcpet_status mcpet_scene_lane_plan(const mcpet_scene* scene, int lane_mode, int histories_per_lane,
+                                   long long capacity, uint32_t* voxel, uint32_t* n_lanes,
+                                   unsigned long long* first_lane, unsigned long long* stream_base,
+                                   double* inv_rate, long long* n_emitters, unsigned long long* total_lanes);
+
 /* ---- asynchronous host-buffer runs --------------------------------------
  *
  * mcpet_run without the wait: the plan upload, zeroing and transport are

@@ -1268,6 +1268,32 @@ void CUDART_CB finish_async(void* p) {
 
 extern "C" {
 
+mcpet_status mcpet_scene_lane_plan(const mcpet_scene* sc, int lane_mode, int histories_per_lane,
+                                   long long capacity, uint32_t* voxel, uint32_t* n_lanes,
+                                   unsigned long long* first_lane, unsigned long long* stream_base,
+                                   double* inv_rate, long long* n_emitters, unsigned long long* total_lanes) {
+  if (!sc || !n_emitters) return set_error(MCPET_ERR_ARG, "null argument");
+  if (lane_mode < 0 || lane_mode > 1) return set_error(MCPET_ERR_ARG, "unknown lane mode %d", lane_mode);
+  const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
+  const int hpl = histories_per_lane > 0 ? histories_per_lane : auto_hpl(sc);
+  std::vector<Emitter> em;
+  uint64_t lanes = 0;
+  mcpet_status s = plan_host(sc, lane_mode, tpb, hpl, em, lanes);
+  if (s != MCPET_OK) return s;
+  *n_emitters = (long long)em.size();
+  if (total_lanes) *total_lanes = lanes;
+  if (capacity < (long long)em.size())
+    return set_error(MCPET_ERR_LIMIT, "lane plan has %zu emitters, capacity %lld", em.size(), capacity);
+  for (size_t i = 0; i < em.size(); ++i) {
+    if (voxel) voxel[i] = em[i].voxel;
+    if (n_lanes) n_lanes[i] = em[i].n_lanes;
+    if (first_lane) first_lane[i] = em[i].first_lane;
+    if (stream_base) stream_base[i] = em[i].stream_base;
+    if (inv_rate) inv_rate[i] = em[i].inv_rate;
+  }
+  return MCPET_OK;
+}
+
 mcpet_status mcpet_run_async(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out) {
   if (!sc || !out) return set_error(MCPET_ERR_ARG, "null argument");
   if (out->psf || out->material_dose || out->voxel_dose)

@@ -204,6 +204,8 @@ _SIGNATURES = {
     "mcpet_run_batch_device": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_device_noalloc": (C.c_int, [P, P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_last_run_guard": (C.c_int, [P, C.POINTER(C.c_ulonglong)]),
+    "mcpet_scene_lane_plan": (C.c_int, [P, C.c_int, C.c_int, C.c_longlong, P, P, P, P, P,
+                                        C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong)]),
     "mcpet_run_async": (C.c_int, [P, C.POINTER(RunOpts), C.POINTER(Tallies)]),
     "mcpet_run_wait": (C.c_int, [P]),
     "mcpet_autotune": (C.c_int, [P, C.c_int, C.POINTER(RunOpts), C.POINTER(Tallies), C.c_double,

@@ -461,6 +461,27 @@ class Scene:
         check(lib().mcpet_run_async(self._h, C.byref(co), C.byref(t)))
         return res
 
+    def lane_plan(self, lane_mode: int = _abi.LANES_BALANCED, histories_per_lane: int = 0) -> dict:
+        """The lane plan a run with these settings uses (mcpet_scene_lane_plan;
+        host only): arrays voxel, n_lanes, first_lane, stream_base, inv_rate in
+        launch order, and the total lane count."""
+        n = C.c_longlong(0)
+        tot = C.c_ulonglong(0)
+        L = lib()
+        st = L.mcpet_scene_lane_plan(self._h, lane_mode, histories_per_lane, 0, None, None, None, None, None,
+                                     C.byref(n), C.byref(tot))
+        if st not in (0, 6):
+            check(st)
+        k = n.value
+        out = {"voxel": np.zeros(k, np.uint32), "n_lanes": np.zeros(k, np.uint32),
+               "first_lane": np.zeros(k, np.uint64), "stream_base": np.zeros(k, np.uint64),
+               "inv_rate": np.zeros(k, np.float64)}
+        check(L.mcpet_scene_lane_plan(self._h, lane_mode, histories_per_lane, k, *[_ptr(out[f]) for f in
+                                      ("voxel", "n_lanes", "first_lane", "stream_base", "inv_rate")],
+                                      C.byref(n), C.byref(tot)))
+        out["total_lanes"] = int(tot.value)
+        return out
+
     def wait(self) -> None:
         """mcpet_run_wait: block until the scene's asynchronous runs are done."""
         check(lib().mcpet_run_wait(self._h))
