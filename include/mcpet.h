@@ -324,7 +324,7 @@ mcpet_status mcpet_scene_lane_plan(const mcpet_scene* scene, int lane_mode, int 
  * stream of the scene's own, and the call returns before any of it has run.
  * The scene alternates between two sets of device tallies, so one run's
  * downloads overlap the next run's transport (two runs of a scene in flight
- * at most; the third waits in stream order for the first's downloads).
+ * at most: the call for a third waits until the first's downloads are done).
  * out's scalar pointers (total_histories, coincidences, psf_count,
  * counters) are written when the downloads finish; out and its buffers must
  * stay valid until then (use pinned host buffers for copies that overlap).

@@ -1312,8 +1312,12 @@ mcpet_status mcpet_run_async(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_
   const int k = d.async_next;
   cudaStream_t st = opts ? (cudaStream_t)opts->stream : nullptr;
   cudaStream_t cs = (cudaStream_t)d.copy_stream;
-  /* set k is free again once its previous download finished */
-  if (d.copied_pending[k]) CUDA_TRY(cudaStreamWaitEvent(st, (cudaEvent_t)d.copied[k], 0));
+  /* set k is free again once its previous download finished; the host waits
+   * too, because that download's host function still reads async_out[k] */
+  if (d.copied_pending[k]) {
+    CUDA_TRY(cudaEventSynchronize((cudaEvent_t)d.copied[k]));
+    CUDA_TRY(cudaStreamWaitEvent(st, (cudaEvent_t)d.copied[k], 0));
+  }
   DeviceTallies O;
   memset(&O, 0, sizeof(O));
   O.trues = k ? d.trues_b : d.trues;
