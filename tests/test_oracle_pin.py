@@ -139,3 +139,18 @@ def test_pin_dose_tallies(workdir):
     np.testing.assert_array_equal(o["material_dose"], r["material_dose"])
     np.testing.assert_array_equal(o["voxel_dose"], r["voxel_dose"])
     sc.close()
+
+
+def test_pin_long_axial_body_phantom(workdir):
+    """The long-axial rings (256 x 4 mm, span 11, MRD 38; a 192-crystal ring with
+    96 x 96 bins keeps the sinograms small) around the body phantom with lungs
+    (0.3 g/cm^3) and bone (1.85 g/cm^3)."""
+    mat, rho, act, vs, used = inputs.body_phantom(shape=(50, 32, 32), voxel_cm=1.6, seed=5, total_bq=2.0e4)
+    scan = inputs.scanner_long_axial(max_ring_difference=38, n_angles=96, n_radial=96)
+    scan["n_crystals"] = 192
+    sc = scenes.scene_from_arrays(workdir, mat, rho, act, vs, tissues=used, seed=606, **scan)
+    assert sc.config.n_sinograms == 3373
+    o, r = _run_both(sc)
+    assert o["trues"].sum() + o["scatter"].sum() > 200
+    _assert_same(o, r)
+    sc.close()
