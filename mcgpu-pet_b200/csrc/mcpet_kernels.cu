@@ -535,7 +535,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
    * and Rayleigh tables of all scenes' materials; shared staging off); the
    * launch's lanes are the scenes' lanes one scene after the other, and each
    * lane reads its scene's parameters, lane plan, tables and tallies from
-   * slots[scene].  kRecord: tallied coincidences are also written to
+   * slots[scene] -- except what kShare marks as the same in every scene
+   * (kShareScanner: detector, sinogram and tally settings; kSharePhantom:
+   * grid, voxel keys, palette and tables), which comes from P and T as in a
+   * single-scene launch.  A batched lane's RANECU start uses P's jump tables
+   * (they do not depend on the scene) with its scene's seed; a thread keeps
+   * its totals for the current scene in the shared per-thread state and adds
+   * them to that scene's when it moves to another.  kRecord: tallied coincidences are also written to
    * O.events for the gradient replay.  kDose: the material and voxel dose
    * tallies are on (O.mat_dose / O.vox_dose, or the slots' in a batch). */
   /* kDevicePlan: the lane plan was built on the device and its size is read
