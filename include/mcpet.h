@@ -329,8 +329,10 @@ mcpet_status mcpet_scene_lane_plan(const mcpet_scene* scene, int lane_mode, int 
  * counters) are written when the downloads finish; out and its buffers must
  * stay valid until then (use pinned host buffers for copies that overlap).
  * No PSF or dose tallies, no transport_ms.  Runs of a scene are ordered on
- * one stream.  mcpet_run_wait blocks until every download of the scene has
- * finished and reports guard trips of those runs as MCPET_ERR_DEVICE.
+ * one stream; until mcpet_run_wait, the scene's other run functions refuse
+ * it (MCPET_ERR_ARG), as they share its run words.  mcpet_run_wait blocks
+ * until every download of the scene has finished and reports guard trips
+ * of those runs as MCPET_ERR_DEVICE.
  * Replaces the reference's blocking launch, synchronisation and downloads
  * (MCGPU-PET.cu:483-535) for callers that run many acquisitions. */
 mcpet_status mcpet_run_async(mcpet_scene* scene, const mcpet_run_opts* opts, mcpet_tallies* out);

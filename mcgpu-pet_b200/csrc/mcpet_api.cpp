@@ -354,6 +354,14 @@ mcpet_status build_lanes(mcpet_scene* sc, int mode, int tpb, int hpl, cudaStream
   return MCPET_OK;
 }
 
+/* Other runs share the scene's run words and first tally set with the
+ * asynchronous runs: they wait for mcpet_run_wait. */
+mcpet_status check_no_async(const mcpet_scene* sc) {
+  if (sc && (sc->dev.copied_pending[0] || sc->dev.copied_pending[1]))
+    return set_error(MCPET_ERR_ARG, "asynchronous runs of this scene are in flight: call mcpet_run_wait first");
+  return MCPET_OK;
+}
+
 mcpet_status ensure_device(mcpet_scene* sc) {
   if (sc->dev.device < 0) return mcpet_scene_to_device(sc, -1);
   CUDA_TRY(cudaSetDevice(sc->dev.device));
@@ -715,6 +723,8 @@ mcpet_status check_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   for (int k = 0; k < n; ++k) {
     if (!scenes[k]) return set_error(MCPET_ERR_ARG, "scene %d of the batch is null", k);
     mcpet_status s = validate_opts(scenes[k], opts);
+    if (s != MCPET_OK) return s;
+    s = check_no_async(scenes[k]);
     if (s != MCPET_OK) return s;
   }
   SharedTables local;
@@ -1139,6 +1149,10 @@ mcpet_status mcpet_scene_to_device(mcpet_scene* sc, int device) {
 }
 
 mcpet_status mcpet_run_device(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out) {
+  {
+    const mcpet_status as_ = check_no_async(sc);
+    if (as_ != MCPET_OK) return as_;
+  }
   if (!sc || !out) return set_error(MCPET_ERR_ARG, "null argument");
   DeviceTallies O;
   memset(&O, 0, sizeof(O));
@@ -1162,6 +1176,10 @@ mcpet_status mcpet_run_device(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet
 }
 
 mcpet_status mcpet_run(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* out) {
+  {
+    const mcpet_status as_ = check_no_async(sc);
+    if (as_ != MCPET_OK) return as_;
+  }
   if (!sc || !out) return set_error(MCPET_ERR_ARG, "null argument");
   mcpet_status s = validate_opts(sc, opts);
   if (s != MCPET_OK) return s;
@@ -1502,6 +1520,8 @@ mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpe
     if (n_scenes != 1 || !scenes || !scenes[0]) return set_error(MCPET_ERR_ARG, "autotune needs at least one scene");
     mcpet_status cs = validate_opts(scenes[0], &o);
     if (cs != MCPET_OK) return cs;
+    cs = check_no_async(scenes[0]);
+    if (cs != MCPET_OK) return cs;
   }
   o.collect_counters = 0;
   const bool balanced = o.lane_mode == MCPET_LANES_BALANCED;
@@ -1669,6 +1689,10 @@ mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcp
 
 mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_tallies* device_out,
                         mcpet_grad_args* g) {
+  {
+    const mcpet_status as_ = check_no_async(sc);
+    if (as_ != MCPET_OK) return as_;
+  }
   if (!sc || !device_out || !g) return set_error(MCPET_ERR_ARG, "null argument");
   if (!g->measured) return set_error(MCPET_ERR_ARG, "the measured sinogram is required");
   if (!device_out->trues || !device_out->scatter)
@@ -1766,6 +1790,10 @@ mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_talli
 
 mcpet_status mcpet_run_psf_stream(mcpet_scene* sc, const mcpet_run_opts* opts, long long chunk_records,
                                   mcpet_psf_sink sink, void* user, mcpet_tallies* out) {
+  {
+    const mcpet_status as_ = check_no_async(sc);
+    if (as_ != MCPET_OK) return as_;
+  }
   if (!sc || !sink || !out) return set_error(MCPET_ERR_ARG, "null argument");
   if (!(sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 1))
     return set_error(MCPET_ERR_ARG, "the scene does not tally a PSF (REPORT PSF/SINOGRAM 0 or 1)");
@@ -1905,6 +1933,10 @@ mcpet_status mcpet_run_psf_stream(mcpet_scene* sc, const mcpet_run_opts* opts, l
 
 mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_device, const mcpet_run_opts* opts,
                                       mcpet_tallies* out) {
+  {
+    const mcpet_status as_ = check_no_async(sc);
+    if (as_ != MCPET_OK) return as_;
+  }
   if (!sc || !activity_device || !out) return set_error(MCPET_ERR_ARG, "null argument");
   const long long nv = (long long)sc->mat0.size();
   if (nv > MCPET_NOALLOC_MAX_VOXELS || nv > kNoAllocMaxVoxels)

@@ -261,6 +261,10 @@ def test_async_runs_equal_blocking_runs(workdir):
             sc.set_activity(a)
             res.append(sc.run_async(b, mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED, seed_override=seed)))
             bufs.append(b)
+        # other runs share the scene's run words: refused until wait()
+        with pytest.raises(mcpet.McpetError) as e:
+            sc.run(mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED))
+        assert e.value.status == 1 and "mcpet_run_wait" in str(e.value)
         sc.wait()
         for k, (w, b, r) in enumerate(zip(want, bufs, res)):
             for key in ("trues", "scatter", "image_trues", "image_scatter", "spectrum"):
