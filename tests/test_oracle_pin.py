@@ -154,3 +154,24 @@ def test_pin_long_axial_body_phantom(workdir):
     assert o["trues"].sum() + o["scatter"].sum() > 200
     _assert_same(o, r)
     sc.close()
+
+
+def test_pin_many_phantom_workload_geometry(workdir):
+    """A phantom of the many-phantom workload (seeded head-like cube at 2-4 mm)
+    in the 32-ring batch scanner, a subset of its emitting voxels."""
+    mat, rho, act, vs, used = next(inputs.batch_phantoms(1, 2.0e5, seed=8))
+    sc = scenes.scene_from_arrays(workdir, mat, rho, act, vs, tissues=used, seed=1000, **inputs.scanner_batch())
+    voxels = np.nonzero(sc.export_tables()["voxels"][:, 2] > 0)[0][::5].astype(np.int32)
+    o, r = _run_both(sc, voxel_list=voxels)
+    assert o["trues"].sum() + o["scatter"].sum() > 100
+    _assert_same(o, r)
+    sc.close()
+
+
+def test_batch_phantoms_shapes():
+    shapes = [(p[0].shape, p[3]) for p in inputs.batch_phantoms(6, 1.0e6, seed=3)]
+    again = [(p[0].shape, p[3]) for p in inputs.batch_phantoms(6, 1.0e6, seed=3)]
+    assert shapes == again
+    for (nz, ny, nx), vs in shapes:
+        assert nz == ny == nx and 32 <= nx <= 192
+        assert 0.0 < vs[0] <= 0.4 + 1e-12 and nx * vs[0] <= 40.0 + 1e-9
