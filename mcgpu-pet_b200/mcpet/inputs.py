@@ -396,8 +396,14 @@ def spec_for(mat_files: List[str], voxel_file: str, **kw) -> InputSpec:
 
 
 def config_from_spec(spec: InputSpec, workdir: str):
-    """Parse an InputSpec through the C ABI (writes a temporary .in)."""
+    """Parse an InputSpec through the C ABI (through a temporary .in file of
+    its own in workdir, so that processes sharing workdir do not collide)."""
+    import tempfile
     from .scene import read_config
-    p = os.path.join(workdir, "_spec.in")
-    write_input(p, spec)
-    return read_config(p)
+    fd, p = tempfile.mkstemp(prefix="_spec_", suffix=".in", dir=workdir)
+    os.close(fd)
+    try:
+        write_input(p, spec)
+        return read_config(p)
+    finally:
+        os.unlink(p)
