@@ -9,9 +9,14 @@ the tallies and runs the full transport of those 1e9 decays (2e9 photons).
 
 Arms:
   default           this library on the GPU(s): device-resident timed steps
-                    (value), plus an end-to-end pass through the host-buffer
-                    C-ABI call mcpet_run (e2e) and the reference's own CPU
+                    (value), plus end-to-end steps through the host-buffer
+                    C-ABI call mcpet_run_async (e2e; the blocking mcpet_run is
+                    timed beside it), the gradient of the sinogram
+                    log-likelihood (gradient), and the reference's own CPU
                     implementation on a bounded sample (cpu_baseline).
+                    --batch-scenes N adds the many-phantom batch, autotuner
+                    and CUDA-graph measurements; --beds N the long-axial body
+                    workload with N bed positions and its gradient.
   --impl reference  the reference's own CPU implementation (its transport
                     kernel compiled for the host, all cores) on bounded
                     samples of the same workload.
