@@ -12,9 +12,14 @@ libref_prog.so).  Every value stored here is produced by the reference code:
 * sample_run.npz    the reference transport on the sample geometry (9^3
                     voxels, seed 12345), host build: tallies as sparse bins;
 * tables.npz        checksums of the interpolation tables built by
-                    load_material for air + water.
+                    load_material for air + water;
+* detector_kat_long_axial.npz  tally_Sinogram on photon pairs spread over
+                    the 1 m long-axial scanner (256 rings, span 11, MRD 255:
+                    bins up to 1.82e9, which the reference's int bin index
+                    still holds).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                # every fixture
+    python tests/golden/make_golden.py long_axial     # only the long-axial one
 """
 from __future__ import annotations
 
@@ -46,8 +51,30 @@ def sha(a) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
+def long_axial(work, ref):
+    rng = np.random.default_rng(20261203)
+    mat, rho, act, vs, used = inputs.body_phantom(shape=(50, 32, 32), voxel_cm=1.6, seed=5, total_bq=1.0e3)
+    kat = {}
+    for blur in (0.0, 0.12):
+        sc = scenes.scene_from_arrays(work, mat, rho, act, vs, tissues=used, energy_resolution=blur,
+                                      **inputs.scanner_long_axial())
+        p = refbind.params_from_scene(sc)
+        ev = scenes.random_events(4000, rng, box=(4.0, 4.0, 100.0), e_range=(360e3, 590e3))
+        out = ref.sinogram_events(p, ev)
+        key = f"res{int(blur * 100)}"
+        for k, v in ev.items():
+            kat[f"{key}_{k}"] = v
+        kat[f"{key}_out"] = out
+        sc.close()
+    np.savez_compressed(os.path.join(HERE, "detector_kat_long_axial.npz"), **kat)
+
+
 def main():
     work = tempfile.mkdtemp()
+    if sys.argv[1:] == ["long_axial"]:
+        long_axial(work, refbind.RefCPU())
+        print("long-axial fixture written to", HERE)
+        return
     ref = refbind.RefCPU()
     ids = np.concatenate([np.arange(0, 64), [1000, 65535, 1 << 20, 33554431, 123456789, 838860799]]).astype(np.int64)
     s, f, d = ref.prng(12345, ids.astype(np.int32), 12)
@@ -86,6 +113,7 @@ def main():
                         pmax=sha(rt.pmax[: io_cfg.n_e, used]), compton=sha(np.concatenate([rt.fco, rt.uico, rt.fj0])),
                         rayleigh=sha(np.concatenate([rt.xco, rt.pco, rt.aco, rt.bco])), voxels=sha(vox),
                         nsinos=io_cfg.nsinos, n_e=io_cfg.n_e)
+    long_axial(work, ref)
     print("golden fixtures written to", HERE)
 
 

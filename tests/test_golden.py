@@ -72,3 +72,25 @@ def test_library_tables_match_golden_checksums(workdir):
     assert _sha(np.concatenate([t["xco"], t["pco"], t["aco"], t["bco"]])) == str(g["rayleigh"])
     assert _sha(t["voxels"]) == str(g["voxels"])
     sc.close()
+
+
+def _long_axial_cases(workdir):
+    g = np.load(os.path.join(GOLD, "detector_kat_long_axial.npz"))
+    mat, rho, act, vs, used = inputs.body_phantom(shape=(50, 32, 32), voxel_cm=1.6, seed=5, total_bq=1.0e3)
+    for blur in (0, 12):
+        ev = {k: g[f"res{blur}_{k}"] for k in ["e2", "e1", "pos2", "pos1", "dir2", "dir1", "st2", "st1", "seeds"]}
+        sc = scenes.scene_from_arrays(workdir, mat, rho, act, vs, tissues=used, energy_resolution=blur / 100.0,
+                                      **inputs.scanner_long_axial())
+        yield blur, sc, ev, g[f"res{blur}_out"]
+
+
+def test_oracle_detector_matches_golden_long_axial(workdir):
+    """The reference's tally_Sinogram on pairs spread over the 1 m scanner
+    (span 11, MRD 255, bins up to 1.82e9): the oracle gives the same bins,
+    classes, spectrum bins and RNG states."""
+    for blur, sc, ev, want in _long_axial_cases(workdir):
+        assert sc.config.n_bins == 12333 * 384 * 384
+        got = pyoracle.detector(pyoracle.OracleScene(sc), ev)
+        np.testing.assert_array_equal(got, want, err_msg=f"blur {blur}")
+        assert (want[:, 0] >= 0).sum() > 500 and want[:, 0].max() > 1_500_000_000
+        sc.close()

@@ -101,3 +101,15 @@ def test_bed_positions_batched_equal_beds_one_by_one(tmp_path):
     assert all(z_mean[k] < z_mean[k + 1] for k in range(3)), z_mean
     for b in beds:
         b.close()
+
+
+def test_long_axial_detector_bins_match_reference_fixture(tmp_path):
+    """The GPU detector model against the reference's own tally_Sinogram on
+    the long-axial scanner (fixture made by tests/golden/make_golden.py)."""
+    from test_golden import _long_axial_cases
+    for blur, sc, ev, want in _long_axial_cases(str(tmp_path)):
+        got = mcpet.probe_detector(sc, ev)
+        same = np.all(got[:, :4] == want[:, :4], axis=1)
+        assert same.mean() >= 0.999, (blur, (~same).sum())
+        assert (got[:, 0] >= 0).sum() > 500
+        sc.close()
