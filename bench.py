@@ -594,12 +594,12 @@ def main():
             "kernel": "transport_kernel" if args.algorithm == "histories" else "transport_events_kernel",
             "kernel_ms": avg_kernel_ms, "algorithmic_bytes_per_launch": b_alg,
             "counters": counters}
-    prof = os.path.join(ROOT, "profiles", "transport_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "transport_traffic_head_1e9.md")
     if os.path.exists(prof):
-        try:
-            roof["traffic"] = json.load(open(prof)).get("dram_bytes_per_launch_full_workload")
-        except Exception:
-            pass
+        import re
+        m = re.search(r"^dram_bytes_per_launch_full_workload:\s*(\d+)\s*$", open(prof).read(), re.M)
+        if m:
+            roof["traffic"] = int(m.group(1))
 
     gradient = None
     if rank == 0 and world == 1 and not args.no_gradient:
