@@ -546,8 +546,11 @@ def main():
         # mcpet_run_async calls (two in flight: one step's downloads overlap
         # the next step's transport); the clock stops after mcpet_run_wait.
         # The blocking mcpet_run of the same step is timed too.
+        # one pinned set: the downloads of consecutive steps are ordered on the
+        # scene's copy stream, so they may land in the same host buffers
         names = (("trues", nb), ("scatter", nb), ("image_trues", nv), ("image_scatter", nv), ("spectrum", ne))
-        pins = [{k: torch.empty(n, dtype=torch.int32, pin_memory=True) for k, n in names} for _ in range(2)]
+        pin = {k: torch.empty(n, dtype=torch.int32, pin_memory=True) for k, n in names}
+        pins = [pin, pin]
         act_pinned = torch.from_numpy(np.ascontiguousarray(act.ravel())).pin_memory()
 
         def e2e_opts(k):
