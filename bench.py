@@ -12,14 +12,17 @@ Arms:
                     (value), plus end-to-end steps through the host-buffer
                     C-ABI call mcpet_run_async (e2e; the blocking mcpet_run is
                     timed beside it), the gradient of the sinogram
-                    log-likelihood (gradient), and the reference's own CPU
-                    implementation on a bounded sample (cpu_baseline).
+                    log-likelihood (gradient), the reference's own CUDA
+                    build on the same input file and GPU (ref_cuda), and the
+                    reference's own CPU implementation on a fixed voxel
+                    sample (cpu_baseline).
                     --batch-scenes N adds the many-phantom batch, autotuner
                     and CUDA-graph measurements; --beds N the long-axial body
                     workload with N bed positions and its gradient.
-  --impl reference  the reference's own CPU implementation (its transport
-                    kernel compiled for the host, all cores) on bounded
-                    samples of the same workload.
+  --impl reference  the reference's own CPU implementation (its loaders and
+                    its transport kernel compiled for the host, all cores;
+                    no part of this library is loaded) on the same fixed
+                    voxel sample of the workload in every step.
 
 Multi-GPU: one process per GPU (torchrun); every rank runs an independent
 replica with its own seed (the transport has no exchange step); value = all
@@ -51,6 +54,12 @@ EMISSIONS = 1.0e9
 PHANTOM_SEED = 2024
 
 
+def bench_config(emissions: float, n_gpus: int) -> dict:
+    """The workload as both arms report it."""
+    return {"workload": WORKLOAD, "emissions_per_step_per_gpu": emissions, "parallelism": f"replicas x{n_gpus}",
+            "l2": "each step zeroes 4.2 GB of sinograms (> 126 MB L2) before the transport"}
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -62,17 +71,21 @@ def load_peaks():
 
 def build_workload(workdir: str, emissions: float, scanner: str = "head"):
     from mcpet import inputs
-    mat, rho, act, vs, used = inputs.head_phantom(shape=(64, 128, 128), voxel_cm=0.2, seed=PHANTOM_SEED,
-                                                  total_bq=emissions)
-    scan = inputs.scanner_for_head()
-    if scanner == "head32":
-        # profiling variant: same phantom and ring pitch, 32 rings, 128x128 bins
-        # (2 x 130 MB of sinograms instead of 2 x 2.1 GB)
-        scan.update(n_rows=32, n_z_slices=63, max_ring_difference=31, n_radial=128, n_angles=256, n_crystals=512,
-                    fov_z=12.8, detector_height=12.8)
-    spec = inputs.spec_for(inputs.tissue_materials(used), "unused.vox", seed=12345, **scan)
+    mat, rho, act, vs, used, scan = inputs.head_workload(emissions, scanner)
+    spec = inputs.spec_for(inputs.tissue_materials(used), "unused.vox", **scan)
     cfg = inputs.config_from_spec(spec, workdir)
     return cfg, mat, rho, act, vs
+
+
+def write_workload_files(workdir: str, emissions: float) -> str:
+    """The head workload as the reference reads it: a .vox phantom and a .in
+    input file (written by the pure-Python writers of mcpet.inputs, which
+    load no library).  Returns the .in path."""
+    from mcpet import inputs
+    mat, rho, act, vs, used, scan = inputs.head_workload(emissions)
+    vox = inputs.write_vox(os.path.join(workdir, "head_workload.vox"), mat, rho, act, vs)
+    spec = inputs.spec_for(inputs.tissue_materials(used), vox, **scan)
+    return inputs.write_input(os.path.join(workdir, "head_workload.in"), spec)
 
 
 class ClockSampler:
@@ -135,39 +148,51 @@ def algorithmic_bytes(counters: dict) -> int:
             8 * counters["majorant_refreshes"] + 8 * counters["tally_increments"])
 
 
-def cpu_reference_sample(cfg, mat, rho, act, vs, seconds: float, seed: int = 7):
-    """Reference transport kernel compiled for the host (all cores) on a
-    random subset of emitting voxels, every lane of each voxel run to the end of
-    the acquisition.  Returns (coincidences/s, cores, description)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    sys.path.insert(0, ROOT)
-    import mcpet
-    import refbind
-    with mcpet.Scene.from_arrays(cfg, mat, rho, act, vs) as sc:
-        t = sc.export_tables()
-        p = refbind.params_from_scene(sc)
-    cores = os.cpu_count() or 1
-    R = refbind.RefCPU()
-    T = refbind.RefTables.from_scene_export(t)
-    emit = np.nonzero(t["voxels"][:, 2] > 1e-7)[0]
-    rng = np.random.default_rng(seed)
-    order = rng.permutation(emit)
-    # calibrate on a small subset, then size the sample to the time budget
-    n0 = min(len(order), max(4 * cores, 64))
-    t0 = time.perf_counter()
-    r0 = R.run(p, t["voxels"], T, block_list=order[:n0].astype(np.int32), n_threads=cores)
-    dt0 = time.perf_counter() - t0
-    n1 = int(min(len(order) - n0, max(cores, n0 * max(0.0, seconds - dt0) / max(dt0, 1e-3))))
-    sel = order[n0:n0 + n1].astype(np.int32)
-    t1 = time.perf_counter()
-    r1 = R.run(p, t["voxels"], T, block_list=sel, n_threads=cores)
-    dt1 = time.perf_counter() - t1
-    coinc = int(r0["trues"].sum() + r0["scatter"].sum() + r1["trues"].sum() + r1["scatter"].sum())
-    rate = coinc / (dt0 + dt1)
-    desc = (f"{n0 + n1} of {len(emit)} emitting voxels drawn at random (seed {seed}), each with the reference's "
-            f"32 lanes run over the full 1 s acquisition; {coinc} coincidences in {dt0 + dt1:.1f} s on {cores} "
-            f"threads (reference MCGPU-PET_kernel.cu compiled for the host with OpenMP)")
-    return rate, cores, desc, coinc, dt0 + dt1
+class ReferenceCPU:
+    """The reference's own CPU path for the workload: its input file, voxel
+    file and material tables loaded by its own read_input / load_voxels /
+    load_material (MCGPU-PET.cu:866-1831, the host code of
+    oracle/_ref/libref_prog.so), and its transport kernel compiled for the
+    host (oracle/_ref/libref_cpu.so, OpenMP over voxel blocks, all host
+    threads).  Nothing of this library is loaded."""
+
+    def __init__(self, in_path: str, workdir: str):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import refbind
+        self.refbind = refbind
+        cfg, self.voxels, self.tables = refbind.RefIO().load(in_path, cwd=workdir)
+        self.params = refbind.Params.from_buffer_copy(cfg)
+        self.cpu = refbind.RefCPU()
+        self.cores = os.cpu_count() or 1
+        emit = np.nonzero(self.voxels[:, 2] > 1e-7)[0]
+        self.n_emitting = len(emit)
+        self.order = np.random.default_rng(7).permutation(emit).astype(np.int32)
+        self.cum = np.cumsum(self.voxels[self.order, 2].astype(np.float64)) * (self.params.acq_ps * 1e-12)
+        self.total_decays = float(self.cum[-1])
+
+    def sample(self, decays: float) -> np.ndarray:
+        """The first voxels of a fixed seeded permutation of the emitting
+        voxels whose expected decays reach `decays`: the same sample in
+        every leg and every step."""
+        n = int(np.searchsorted(self.cum, decays)) + 1
+        return self.order[:min(n, len(self.order))]
+
+    def run(self, blocks: np.ndarray):
+        t0 = time.perf_counter()
+        r = self.cpu.run(self.params, self.voxels, self.tables, block_list=blocks, n_threads=self.cores)
+        dt = time.perf_counter() - t0
+        return int(r["trues"].sum(dtype=np.int64) + r["scatter"].sum(dtype=np.int64)), dt
+
+    def describe(self, blocks: np.ndarray, coinc: int, secs: float) -> str:
+        decays = float(self.cum[len(blocks) - 1])
+        return (f"{len(blocks)} of {self.n_emitting} emitting voxels (a fixed seeded sample, {decays:.3g} of the "
+                f"workload's {self.total_decays:.3g} expected decays), each with the reference's "
+                f"{self.params.tpb} lanes over the full {self.params.acq_ps * 1e-12:g} s acquisition; {coinc} "
+                f"coincidences in {secs:.1f} s on {self.cores} threads (the reference's read_input / load_voxels / "
+                f"load_material and its MCGPU-PET_kernel.cu compiled for the host with OpenMP)")
+
+
+CPU_SAMPLE_DECAYS = 6.0e7     # 6 % of the head workload per CPU step (~5 s on 16 host threads)
 
 
 def run_reference_arm(args):
@@ -175,27 +200,48 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     with tempfile.TemporaryDirectory() as tmp:
-        cfg, mat, rho, act, vs = build_workload(tmp, args.emissions)
-        per_step = max(5.0, args.cpu_seconds / max(1, args.steps))
+        ref = ReferenceCPU(write_workload_files(tmp, args.emissions), tmp)
+        small = ref.sample(CPU_SAMPLE_DECAYS / 25)
         for _ in range(args.warmup):
-            cpu_reference_sample(cfg, mat, rho, act, vs, min(per_step, 5.0), seed=1)
-        rates, coinc, secs = [], 0, 0.0
-        desc, cores = "", 1
-        for k in range(args.steps):
-            rate, cores, desc, c, s = cpu_reference_sample(cfg, mat, rho, act, vs, per_step, seed=100 + k)
-            rates.append(rate)
+            ref.run(small)
+        blocks = ref.sample(args.cpu_sample_decays)
+        coinc, secs = 0, 0.0
+        for _ in range(args.steps):
+            c, s = ref.run(blocks)
             coinc += c
             secs += s
+        desc = ref.describe(blocks, coinc // max(args.steps, 1), secs / max(args.steps, 1))
+        cores = ref.cores
     value = coinc / secs
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded phantom; random voxel samples of the workload)",
-            "config": {"workload": WORKLOAD, "arm": "reference CPU implementation (host build of its kernel)"},
+            "data": "synthetic (seeded phantom; a fixed voxel sample of the workload per step)",
+            "config": bench_config(args.emissions, args.gpus),
+            "impl_config": {"arm": "reference CPU implementation (its loaders and its kernel compiled for the host)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def measure_reference_cuda(workdir: str, emissions: float) -> dict:
+    """The reference's own CUDA build on this GPU, same workload: its
+    read_input / load_voxels / load_material / init_CUDA_device and one
+    track_particles launch timed with CUDA events (MCGPU-PET.cu:228-535,
+    oracle/_ref/libref_prog.so); coincidences = sum of its trues and
+    scatter sinograms (MCGPU-PET.cu:793-794)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import refbind
+    in_path = write_workload_files(workdir, emissions)
+    cfg, vox, _ = refbind.RefIO().load(in_path, cwd=workdir)
+    nvox = cfg.nx * cfg.ny * cfg.nz
+    r = refbind.RefProg().run(in_path, cfg.nbins, nvox, cfg.ne, cwd=workdir)
+    coinc = int(r["trues"].sum(dtype=np.int64) + r["scatter"].sum(dtype=np.int64))
+    return {"kernel_ms": r["kernel_ms"], "coincidences": coinc, "value": coinc / (r["kernel_ms"] * 1e-3),
+            "unit": UNIT, "histories": r["total_histories"],
+            "what": "reference CUDA build (its own loaders and track_particles launch, reference lanes, seed 12345), "
+                    "kernel time from CUDA events on this GPU"}
 
 
 def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, replays: int = 3) -> dict:
@@ -430,7 +476,10 @@ def main():
     ap.add_argument("--impl", default="mcpet", choices=["mcpet", "reference"])
     ap.add_argument("--emissions", type=float, default=EMISSIONS)
     ap.add_argument("--lanes", default="balanced", choices=["balanced", "reference"])
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-sample-decays", type=float, default=CPU_SAMPLE_DECAYS,
+                    help="expected decays of the fixed voxel sample each CPU step runs")
+    ap.add_argument("--no-ref-cuda", action="store_true",
+                    help="skip the reference CUDA build's run of the workload (ref_cuda)")
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--algorithm", default="auto", choices=["auto", "histories", "events"])
@@ -619,24 +668,35 @@ def main():
         torch.cuda.empty_cache()
         beds = measure_beds(args.beds, tmp)
 
+    ref_cuda = None
+    if rank == 0 and world == 1 and not args.no_ref_cuda and args.scanner == "head":
+        ref_cuda = measure_reference_cuda(tmp, args.emissions)
+        ref_cuda["this_library_kernel_ms"] = avg_kernel_ms
+        ref_cuda["kernel_time_ratio"] = ref_cuda["kernel_ms"] / avg_kernel_ms
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, desc, _, _ = cpu_reference_sample(cfg, mat, rho, act, vs, args.cpu_seconds)
-        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+        ref = ReferenceCPU(write_workload_files(tmp, args.emissions), tmp)
+        blocks = ref.sample(args.cpu_sample_decays)
+        ref.run(ref.sample(args.cpu_sample_decays / 25))          # warm-up
+        c, secs = ref.run(blocks)
+        cpu = {"value": c / secs, "unit": UNIT, "cores": ref.cores, "kind": "reference",
+               "sample": ref.describe(blocks, c, secs)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded head phantom; tissue densities on the reference's own air/water material tables)",
-                "config": {"workload": WORKLOAD, "emissions_per_step_per_gpu": args.emissions,
-                           "lanes": args.lanes, "algorithm": args.algorithm, "parallelism": f"replicas x{world}",
-                           "block_threads": args.block_threads or "auto",
-                           "histories_per_lane": args.histories_per_lane or "auto",
-                           "l2": "each step zeroes 4.2 GB of sinograms (> 126 MB L2) before the kernel",
-                           "coincidences_per_step": total / args.steps / world, "histories_last_step": hist,
-                           "guard_trips": guard},
+                "config": bench_config(args.emissions, world),
+                "impl_config": {"lanes": args.lanes, "algorithm": args.algorithm,
+                                "block_threads": args.block_threads or "auto",
+                                "histories_per_lane": args.histories_per_lane or "auto"},
+                "run": {"coincidences_per_step": total / args.steps / world, "histories_last_step": hist,
+                        "guard_trips": guard},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks}
+        if ref_cuda is not None:
+            line["ref_cuda"] = ref_cuda
         if gradient is not None:
             line["gradient"] = gradient
         if batch is not None:

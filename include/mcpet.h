@@ -129,6 +129,15 @@ typedef struct {
   void* stream;                   /* cudaStream_t; NULL = default stream */
   int algorithm;                  /* 0 automatic, 1 history loop per thread, 2 warp-regrouped event loop
                                      (same results, different schedule) */
+  /* Device loop guards.  The reference's Woodcock loop and the rejection
+   * loops of GCOa / GRAa are unbounded (MCGPU-PET_kernel.cu:319-342, 1247,
+   * 1390-1526); here a photon that takes more Woodcock steps, or more
+   * iterations in one rejection loop, than these caps is dropped and counted
+   * as a guard trip (the run then returns MCPET_ERR_DEVICE).  <= 0: the
+   * defaults, 2^20 steps and 2^16 iterations, which physical input never
+   * reaches. */
+  int max_woodcock_steps;
+  int max_rejections;
 } mcpet_run_opts;
 
 /* Event counters (when collect_counters=1). */
@@ -413,14 +422,23 @@ void mcpet_batch_graph_destroy(mcpet_batch_graph* graph);
  * device share that array and rewrite it, so calls that overlap on the GPU
  * (several streams or threads at once) race; serialise them.  The first call
  * on a device looks up the array's device address; make that first call
- * before any stream capture.  Lanes are laid out in voxel order: with
- * MCPET_LANES_REFERENCE the results equal mcpet_run_device's.  Guard trips
- * are reported only through device_out->counters (collect_counters=1). */
+ * before any stream capture.  The address is kept for the life of the
+ * device's context: do not use this entry point across a cudaDeviceReset.
+ * Lanes are laid out in voxel order: with MCPET_LANES_REFERENCE the results
+ * equal mcpet_run_device's; with balanced lanes and histories_per_lane <= 0
+ * the automatic lane size is computed on the device from activity_device.
+ * A plan whose RANECU stream ids would reach 2^31 (the reference's 31-bit
+ * thread ids) runs nothing and counts one guard trip.  Guard trips (that
+ * one, and the transport's loop caps) are reported in
+ * device_out->counters->guard_trips when collect_counters=1, and by
+ * mcpet_last_run_guard(scene) after the call (a blocking read of the static
+ * array, which allocates nothing). */
 #define MCPET_NOALLOC_MAX_VOXELS (1 << 20)
 mcpet_status mcpet_run_device_noalloc(mcpet_scene* scene, const float* activity_device,
                                       const mcpet_run_opts* opts, mcpet_tallies* device_out);
 
-/* Device-side guard status of the last run on this scene (blocking read). */
+/* Device-side guard status of the last run on this scene (blocking read);
+ * after mcpet_run_device_noalloc, that call's trips. */
 mcpet_status mcpet_last_run_guard(mcpet_scene* scene, unsigned long long* trips);
 
 /* ---- outputs ----------------------------------------------------------- */

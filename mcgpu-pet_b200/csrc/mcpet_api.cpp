@@ -46,6 +46,9 @@ void dfree(T*& p) {
   p = nullptr;
 }
 
+constexpr int kMaxStepsDefault = 1 << 20;       /* Woodcock steps per photon */
+constexpr int kMaxRejectionsDefault = 1 << 16;  /* iterations per sampler rejection loop */
+
 /* (a^e) mod m with exact 64-bit arithmetic. */
 uint32_t powmod(uint64_t a, uint64_t e, uint64_t m) {
   uint64_t r = 1 % m;
@@ -143,6 +146,14 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 32, 1, 32);
   P.step_keep = env_int("MCPET_STEP_KEEP", 2, 1, 8);
   P.quorum_rayleigh = env_int("MCPET_QUORUM_RAYLEIGH", 2, 1, 32);
+  P.max_steps = kMaxStepsDefault;
+  P.max_rejections = kMaxRejectionsDefault;
+}
+
+/* loop caps of a run: the options' values, or the defaults */
+void apply_caps(const mcpet_run_opts& o, TransportParams& P) {
+  P.max_steps = o.max_woodcock_steps > 0 ? o.max_woodcock_steps : kMaxStepsDefault;
+  P.max_rejections = o.max_rejections > 0 ? o.max_rejections : kMaxRejectionsDefault;
 }
 
 mcpet_status upload_tables(mcpet_scene* sc) {
@@ -412,6 +423,7 @@ mcpet_status prepare_params(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTall
   if (o.seed_override != 0) P.seed = o.seed_override;
   if (P.seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", P.seed);
   P.background_mode = o.background_mode ? 1 : 0;
+  apply_caps(o, P);
   if (!O.psf) P.psf_capacity = 0;
 
   const bool sino = sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 2;
@@ -485,6 +497,7 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   P.n_emitters = sc->dev.n_emitters;
 
   auto& d = sc->dev;
+  d.last_run_noalloc = false;
   unsigned long long* small = d.small;
   O.guard = small + 0;
   O.lane_cursor = small + 1;
@@ -962,6 +975,7 @@ mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_op
   bind_blob(L, dbuf);
   auto& d = s0->dev;
   /* the launch's guard and work queue are scene 0's words */
+  for (int k = 0; k < n; ++k) scenes[k]->dev.last_run_noalloc = false;
   for (int k = 1; k < n; ++k) CUDA_TRY(cudaMemsetAsync(scenes[k]->dev.small, 0, sizeof(unsigned long long), st));
   s = enqueue_batch_launch(scenes, n, L, dbuf, d.small + 0, d.small + 1, st,
                            ms_out ? (cudaEvent_t)d.ev0 : nullptr, ms_out ? (cudaEvent_t)d.ev1 : nullptr);
@@ -1836,6 +1850,7 @@ mcpet_status mcpet_run_psf_stream(mcpet_scene* sc, const mcpet_run_opts* opts, l
   if (s != MCPET_OK) return s;
   O.guard = d.small + 0;
   O.lane_cursor = d.small + 1;
+  d.last_run_noalloc = false;
   CUDA_TRY(cudaMemsetAsync(d.small, 0, 2 * sizeof(unsigned long long), st));
   if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
   if (!d.gwords) CUDA_TRY(dmalloc(&d.gwords, 4 * sizeof(unsigned long long)));
@@ -1961,11 +1976,13 @@ mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_dev
   fill_params(sc, P);
   if (o.seed_override != 0) P.seed = o.seed_override;
   P.background_mode = o.background_mode ? 1 : 0;
+  apply_caps(o, P);
   if (!out->psf) P.psf_capacity = 0;
   else P.psf_capacity = (int)std::min<long long>(out->psf_capacity, 0x7fffffff);
   if (!sino) P.spectrum_in_shared = 0;
   const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
-  int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
+  /* <= 0: automatic, from the caller's activity map on the device */
+  const int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : 0;
 
   DeviceTallies O;
   memset(&O, 0, sizeof(O));
@@ -1999,8 +2016,9 @@ mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_dev
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   const int grid = d.sm_count * bps;
-  CUDA_TRY(launch_transport_noalloc(P, device_tables(sc), O, activity_device, o.lane_mode, tpb, hpl, counters,
-                                    grid, block, smem, st));
+  d.last_run_noalloc = true;
+  CUDA_TRY(launch_transport_noalloc(P, device_tables(sc), O, activity_device, o.lane_mode, tpb, hpl, d.sm_count,
+                                    counters, grid, block, smem, st));
   return MCPET_OK;
 }
 
@@ -2011,7 +2029,8 @@ mcpet_status mcpet_last_run_guard(mcpet_scene* sc, unsigned long long* trips) {
     return MCPET_OK;
   }
   CUDA_TRY(cudaSetDevice(sc->dev.device));
-  CUDA_TRY(cudaMemcpy(trips, sc->dev.small, 8, cudaMemcpyDeviceToHost));
+  if (sc->dev.last_run_noalloc) CUDA_TRY(noalloc_guard_trips(trips));
+  else CUDA_TRY(cudaMemcpy(trips, sc->dev.small, 8, cudaMemcpyDeviceToHost));
   return MCPET_OK;
 }
 

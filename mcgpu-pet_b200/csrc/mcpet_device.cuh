@@ -22,7 +22,8 @@ constexpr double kPi = 3.14159265358979323846;   /* PI */
 constexpr float kAnnihilation = 510998.95f;      /* ANNIHILATION_PHOTON_ENERGY */
 constexpr double kInvLightSpeed = (1.0 / 29979245800e-12); /* ps per cm */
 
-/* Loop guards: far above anything a physical history reaches; when one
+/* Loop guards (defaults of mcpet_run_opts.max_woodcock_steps and
+ * max_rejections): far above anything a physical history reaches; when one
  * fires the photon is dropped and the run reports MCPET_ERR_DEVICE. */
 constexpr int kMaxWoodcockSteps = 1 << 20;
 constexpr int kMaxRejections = 1 << 16;
@@ -203,19 +204,20 @@ __device__ __forceinline__ void rotate(float3& d, double costh, double phi) {
  * plus rejection (PENELOPE 2006 GRAa; MCGPU-PET_kernel.cu:1231-1296).
  * Returns false when the rejection guard fired. */
 __device__ __forceinline__ bool sample_rayleigh(Rng& r, float energy, int mat, float pmax,
-                                                const RayleighRows& R, double& costh) {
+                                                const RayleighRows& R, double& costh,
+                                                int max_rejections = kMaxRejections) {
   const int base = mat * kNpRayleigh;
   double xmax = ((double)energy) * 8.065535669099010e-5;
   double xlast = (double)__ldg(&R.xco[base + kNpRayleigh - 1]);
   double x2max = ((xmax * xmax) < xlast) ? (xmax * xmax) : xlast;
   if (xmax < 0.01) {
-    for (int it = 0; it < kMaxRejections; ++it) {
+    for (int it = 0; it < max_rejections; ++it) {
       costh = 1.0 - ranecu_double(r) * 2.0;
       if (!(ranecu_double(r) > ((costh * costh + 1.0) * 0.5))) return true;
     }
     return false;
   }
-  for (int it = 0; it < kMaxRejections; ++it) {
+  for (int it = 0; it < max_rejections; ++it) {
     double ru = ranecu_double(r) * (double)pmax;
     int itn = (int)(ru * (kNpRayleigh - 1));
     int lo = (int)__ldg(&R.itl[itn + base]);
@@ -277,7 +279,8 @@ __device__ __forceinline__ float compton_s0(float E, int mat, const ComptonTable
 
 template <typename Scratch>
 __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, const ComptonTable& C,
-                                               Scratch rn, double& costh, const float* s0_annihilation = nullptr) {
+                                               Scratch rn, double& costh, const float* s0_annihilation = nullptr,
+                                               int max_rejections = kMaxRejections) {
   const float E = energy;
   const int nsh = C.noscco[mat];
   float ek = E * 1.956951306108245e-6f;
@@ -292,7 +295,7 @@ __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, c
   double cdt1;
   int it = 0;
   for (;;) {
-    if (++it > kMaxRejections) return false;
+    if (++it > max_rejections) return false;
     if (ranecu(r) * (a1 + 2. * ek * (ek + 1.f) * taumin * taumin) < a1) {
       tau = powf(taumin, ranecu(r));
     } else {
@@ -333,7 +336,7 @@ __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, c
   float pzomc, af;
   it = 0;
   for (;;) {
-    if (++it > kMaxRejections) return false;
+    if (++it > max_rejections) return false;
     float t = s * ranecu(r);
     float pac = 0.0f;
     int ish = nsh - 1;

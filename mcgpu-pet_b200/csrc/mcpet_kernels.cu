@@ -144,7 +144,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       ph.pos.z += step * ph.dir.z;
       vox = locate(P, ph.pos.x, ph.pos.y, ph.pos.z);
       if (vox < 0) break;
-      if ((unsigned long long)vox >= (unsigned long long)P.n_voxels || ++steps > kMaxWoodcockSteps) {
+      if ((unsigned long long)vox >= (unsigned long long)P.n_voxels || ++steps > P.max_steps) {
         Counting<true>::add(cnt.guard, 1);
         ph.energy = energy;
         return false;
@@ -172,7 +172,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       /* Compton */
       double costh;
       const float e_before = energy;
-      if (!sample_compton(rng, energy, mat0, C, rn, costh)) {
+      if (!sample_compton(rng, energy, mat0, C, rn, costh, nullptr, P.max_rejections)) {
         Counting<true>::add(cnt.guard, 1);
         ph.energy = energy;
         return false;
@@ -193,7 +193,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       if (randno < prob) {
         /* Rayleigh */
         double costh;
-        if (!sample_rayleigh(rng, energy, mat0, rec_hi.z, T.rayleigh, costh)) {
+        if (!sample_rayleigh(rng, energy, mat0, rec_hi.z, T.rayleigh, costh, P.max_rejections)) {
           Counting<true>::add(cnt.guard, 1);
           ph.energy = energy;
           return false;
@@ -677,9 +677,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
         bool ok;
         float e = ph.energy;
         if (is_compton) {
-          ok = sample_compton(rng, e, mat0, cmp, rn, costh, s0_ann);
+          ok = sample_compton(rng, e, mat0, cmp, rn, costh, s0_ann, P.max_rejections);
         } else {
-          ok = sample_rayleigh(rng, e, mat0, kBatch ? cold.f(kCPmax) : rec_hi.z, T.rayleigh, costh);
+          ok = sample_rayleigh(rng, e, mat0, kBatch ? cold.f(kCPmax) : rec_hi.z, T.rayleigh, costh, P.max_rejections);
         }
         if (!ok) {
           Counting<true>::add(cnt.guard, 1);
@@ -850,7 +850,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             if (vox < 0) {
               escaped = true;
               phase = kPhEnd;
-            } else if ((unsigned long long)vox >= (unsigned long long)PG.n_voxels || ++steps > kMaxWoodcockSteps) {
+            } else if ((unsigned long long)vox >= (unsigned long long)PG.n_voxels || ++steps > P.max_steps) {
               Counting<true>::add(cnt.guard, 1);
               escaped = false;
               phase = kPhEnd;
@@ -1185,10 +1185,22 @@ __global__ void __launch_bounds__(256) loglik_kernel(long long nbins, const floa
 constexpr int kPlanChunk = 4096;                                  /* voxels per plan block */
 constexpr int kPlanMaxChunks = kNoAllocMaxVoxels / kPlanChunk;
 
+/* header words */
+enum : int {
+  kHdrCursor = 0,       /* lane work queue */
+  kHdrGuard = 1,        /* guard trips of the call (plan limit + transport guards) */
+  kHdrLanes = 2,        /* lanes of the plan (kernel reads [2], [3]) */
+  kHdrEmitters = 3,
+  kHdrCoinc = 4,        /* coincidence counter when the caller passes none */
+  kHdrHpl = 5,          /* decays per balanced lane used by the plan */
+};
+
 struct NoAllocScratch {
-  unsigned long long header[8];   /* 0 lane cursor, 1 guard, 2 lanes, 3 emitters, 4 coincidences (fallback) */
+  unsigned long long header[8];
   unsigned long long chunk_lanes[kPlanMaxChunks];
   unsigned int chunk_emitters[kPlanMaxChunks];
+  int chunk_last_voxel[kPlanMaxChunks];    /* highest emitting voxel of the chunk, -1 if none */
+  double chunk_activity[kPlanMaxChunks];   /* activity of the chunk's emitting voxels */
   Emitter plan[kNoAllocMaxVoxels];
 };
 
@@ -1198,7 +1210,8 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocS
 
 namespace {
 
-__device__ __forceinline__ unsigned long long plan_lanes_of(float a, int mode, int tpb, double t_s, int hpl) {
+__device__ __forceinline__ unsigned long long plan_lanes_of(float a, int mode, int tpb, double t_s,
+                                                            unsigned long long hpl) {
   if (mode == 0) return (unsigned long long)tpb;
   double L = ceil((double)a * t_s / (double)hpl);
   if (L < 1) L = 1;
@@ -1206,47 +1219,97 @@ __device__ __forceinline__ unsigned long long plan_lanes_of(float a, int mode, i
   return (unsigned long long)L;
 }
 
-/* per chunk of voxels: number of emitters and of lanes */
-__global__ void plan_count_kernel(const float* act, int nvox, int mode, int tpb, double t_s, int hpl,
-                                  NoAllocScratch* S) {
-  __shared__ unsigned long long sl[32];
+/* per chunk of voxels: emitters, their activity and the last emitting voxel */
+__global__ void plan_count_kernel(const float* act, int nvox, NoAllocScratch* S) {
+  __shared__ double sa[32];
   __shared__ unsigned int se[32];
+  __shared__ int sv[32];
   const int v0 = blockIdx.x * kPlanChunk, v1 = min(v0 + kPlanChunk, nvox);
   unsigned int ne = 0;
-  unsigned long long nl = 0;
+  double asum = 0.0;
+  int vlast = -1;
   for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
     float a = act[v];
     if (a > 1.0e-7f) {
       ne += 1;
-      nl += plan_lanes_of(a, mode, tpb, t_s, hpl);
+      asum += (double)a;
+      vlast = v;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
     ne += __shfl_down_sync(0xffffffffu, ne, o);
-    nl += __shfl_down_sync(0xffffffffu, nl, o);
+    asum += __shfl_down_sync(0xffffffffu, asum, o);
+    vlast = max(vlast, __shfl_down_sync(0xffffffffu, vlast, o));
   }
   if ((threadIdx.x & 31) == 0) {
     se[threadIdx.x >> 5] = ne;
-    sl[threadIdx.x >> 5] = nl;
+    sa[threadIdx.x >> 5] = asum;
+    sv[threadIdx.x >> 5] = vlast;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned int te = 0;
-    unsigned long long tl = 0;
+    double ta = 0.0;
+    int tv = -1;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       te += se[w];
-      tl += sl[w];
+      ta += sa[w];
+      tv = max(tv, sv[w]);
     }
     S->chunk_emitters[blockIdx.x] = te;
+    S->chunk_activity[blockIdx.x] = ta;
+    S->chunk_last_voxel[blockIdx.x] = tv;
+  }
+}
+
+/* decays per balanced lane: the caller's value, or the automatic one from
+ * the activity map on the device (expected decays over 3 lanes per
+ * resident thread, clamped to [1, 4096]) */
+__global__ void plan_hpl_kernel(int n_chunks, double t_s, int hpl, double resident_threads, NoAllocScratch* S) {
+  if (threadIdx.x != 0) return;
+  unsigned long long h = (unsigned long long)(hpl > 0 ? hpl : 1);
+  if (hpl <= 0) {
+    double A = 0.0;
+    for (int c = 0; c < n_chunks; ++c) A += S->chunk_activity[c];
+    double x = A * t_s / (resident_threads * 3.0);
+    if (x < 1) x = 1;
+    if (x > 4096) x = 4096;
+    h = (unsigned long long)(int)x;
+  }
+  S->header[kHdrHpl] = h;
+}
+
+/* per chunk of voxels: lanes */
+__global__ void plan_lanes_kernel(const float* act, int nvox, int mode, int tpb, double t_s, NoAllocScratch* S) {
+  __shared__ unsigned long long sl[32];
+  const unsigned long long hpl = S->header[kHdrHpl];
+  const int v0 = blockIdx.x * kPlanChunk, v1 = min(v0 + kPlanChunk, nvox);
+  unsigned long long nl = 0;
+  for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+    float a = act[v];
+    if (a > 1.0e-7f) nl += plan_lanes_of(a, mode, tpb, t_s, hpl);
+  }
+  for (int o = 16; o > 0; o >>= 1) nl += __shfl_down_sync(0xffffffffu, nl, o);
+  if ((threadIdx.x & 31) == 0) sl[threadIdx.x >> 5] = nl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tl = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tl += sl[w];
     S->chunk_lanes[blockIdx.x] = tl;
   }
 }
 
-/* exclusive prefix over the chunks, totals, and the words that start at zero */
-__global__ void plan_scan_kernel(int n_chunks, NoAllocScratch* S) {
+/* Exclusive prefix over the chunks, totals, and the words that start at
+ * zero.  A plan whose RANECU streams reach 2^31 (the reference's 31-bit
+ * thread ids; stream = lane index for balanced lanes, voxel *
+ * threads_per_block + thread for reference lanes) runs nothing: the call
+ * counts a guard trip, in its guard word and, when counters are collected,
+ * in counters[9]. */
+__global__ void plan_scan_kernel(int n_chunks, int mode, int tpb, NoAllocScratch* S, unsigned long long* counters) {
   if (threadIdx.x != 0) return;
   unsigned long long lanes = 0;
   unsigned int emitters = 0;
+  int last = -1;
   for (int c = 0; c < n_chunks; ++c) {
     unsigned long long l = S->chunk_lanes[c];
     unsigned int e = S->chunk_emitters[c];
@@ -1254,28 +1317,31 @@ __global__ void plan_scan_kernel(int n_chunks, NoAllocScratch* S) {
     S->chunk_emitters[c] = emitters;
     lanes += l;
     emitters += e;
+    last = max(last, S->chunk_last_voxel[c]);
   }
-  S->header[0] = 0;      /* lane cursor */
-  S->header[1] = 0;      /* guard trips */
-  S->header[4] = 0;      /* coincidence fallback counter */
-  if (lanes >= (1ull << 31)) {
-    /* more RANECU streams than the reference's 31-bit thread ids: run nothing
-     * and count a guard trip */
-    S->header[1] = 1;
+  S->header[kHdrCursor] = 0;
+  S->header[kHdrGuard] = 0;
+  S->header[kHdrCoinc] = 0;
+  const unsigned long long streams =
+      (mode == 0) ? (last < 0 ? 0ull : ((unsigned long long)last + 1) * (unsigned long long)tpb) : lanes;
+  if (streams >= (1ull << 31)) {
+    S->header[kHdrGuard] = 1;
+    if (counters) counters[9] += 1;
     lanes = 0;
     emitters = 0;
   }
-  S->header[2] = lanes;
-  S->header[3] = emitters;
+  S->header[kHdrLanes] = lanes;
+  S->header[kHdrEmitters] = emitters;
 }
 
 /* emitter records in voxel order (one block per chunk, block-wide scans) */
-__global__ void plan_fill_kernel(const float* act, int nvox, int mode, int tpb, double t_s, int hpl,
-                                 NoAllocScratch* S) {
+__global__ void plan_fill_kernel(const float* act, int nvox, int mode, int tpb, double t_s, NoAllocScratch* S) {
   __shared__ unsigned int we[32];
   __shared__ unsigned long long wl[32];
   __shared__ unsigned int run_e;
   __shared__ unsigned long long run_l;
+  const unsigned long long hpl = S->header[kHdrHpl];
+  if (S->header[kHdrLanes] == 0) return;   /* empty or refused plan */
   const int c = blockIdx.x;
   const int v0 = c * kPlanChunk, v1 = min(v0 + kPlanChunk, nvox);
   if (threadIdx.x == 0) {
@@ -1520,7 +1586,11 @@ cudaError_t launch_advance_seeds(SceneSlot* slots, int n_slots, int step, cudaSt
 }
 
 /* Device address of the scratch array, looked up once per device with that
- * device current (the array's host-side name is only a stand-in). */
+ * device current (the array's host-side name is only a stand-in).  The
+ * address stays valid for the life of the device's primary context; after a
+ * cudaDeviceReset the module may be loaded elsewhere and the cached address
+ * is stale, so the allocation-free entry point must not be used across a
+ * device reset. */
 static std::mutex g_scratch_mutex;
 static void* g_scratch_ptr[128];
 
@@ -1541,8 +1611,8 @@ static cudaError_t noalloc_scratch(NoAllocScratch** out) {
 }
 
 cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,
-                                     const float* activity, int lane_mode, int tpb, int hpl, bool counters,
-                                     int grid, int block, size_t smem, cudaStream_t stream) {
+                                     const float* activity, int lane_mode, int tpb, int hpl, int sm_count,
+                                     bool counters, int grid, int block, size_t smem, cudaStream_t stream) {
   NoAllocScratch* S = nullptr;
   cudaError_t e = noalloc_scratch(&S);
   if (e != cudaSuccess) return e;
@@ -1550,16 +1620,19 @@ cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, D
   if (nvox <= 0 || nvox > kNoAllocMaxVoxels) return cudaErrorInvalidValue;
   const int n_chunks = (nvox + kPlanChunk - 1) / kPlanChunk;
   const double t_s = (double)P.acq_ps * 1e-12;
-  plan_count_kernel<<<n_chunks, 256, 0, stream>>>(activity, nvox, lane_mode, tpb, t_s, hpl, S);
-  plan_scan_kernel<<<1, 32, 0, stream>>>(n_chunks, S);
-  plan_fill_kernel<<<n_chunks, 256, 0, stream>>>(activity, nvox, lane_mode, tpb, t_s, hpl, S);
+  unsigned long long* cnt = counters ? O.counters : nullptr;
+  plan_count_kernel<<<n_chunks, 256, 0, stream>>>(activity, nvox, S);
+  plan_hpl_kernel<<<1, 32, 0, stream>>>(n_chunks, t_s, hpl, (double)sm_count * 2048.0, S);
+  plan_lanes_kernel<<<n_chunks, 256, 0, stream>>>(activity, nvox, lane_mode, tpb, t_s, S);
+  plan_scan_kernel<<<1, 32, 0, stream>>>(n_chunks, lane_mode, tpb, S, cnt);
+  plan_fill_kernel<<<n_chunks, 256, 0, stream>>>(activity, nvox, lane_mode, tpb, t_s, S);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   T.emitters = S->plan;
-  O.lane_cursor = &S->header[0];
-  O.guard = &S->header[1];
-  O.plan_counts = &S->header[2];
-  if (!O.coincidences) O.coincidences = &S->header[4];
+  O.lane_cursor = &S->header[kHdrCursor];
+  O.guard = &S->header[kHdrGuard];
+  O.plan_counts = &S->header[kHdrLanes];
+  if (!O.coincidences) O.coincidences = &S->header[kHdrCoinc];
   if (counters) {
     e = occupancy_smem_attr(transport_events_kernel<true, kEventBlocks, true>, smem);
     if (e == cudaSuccess) transport_events_kernel<true, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
@@ -1569,6 +1642,15 @@ cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, D
   }
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
+}
+
+/* Guard trips of the last allocation-free call on the current device (a
+ * blocking 8-byte read of the scratch header; allocates nothing). */
+cudaError_t noalloc_guard_trips(unsigned long long* trips) {
+  NoAllocScratch* S = nullptr;
+  cudaError_t e = noalloc_scratch(&S);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(trips, &S->header[kHdrGuard], sizeof(unsigned long long), cudaMemcpyDeviceToHost);
 }
 
 cudaError_t launch_grad_replay(const TransportParams& P, const DeviceTables& T, const uint32_t* events,

@@ -41,8 +41,10 @@ cudaError_t launch_advance_seeds(SceneSlot* slots, int n_slots, int step, cudaSt
 /* allocation-free runs: lane plan and work-queue words in a static device array */
 constexpr int kNoAllocMaxVoxels = 1 << 20;
 cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,
-                                     const float* activity, int lane_mode, int tpb, int hpl, bool counters,
-                                     int grid, int block, size_t smem, cudaStream_t stream);
+                                     const float* activity, int lane_mode, int tpb, int hpl, int sm_count,
+                                     bool counters, int grid, int block, size_t smem, cudaStream_t stream);
+/* guard trips of the last allocation-free call on the current device */
+cudaError_t noalloc_guard_trips(unsigned long long* trips);
 
 /* gradient of the sinogram log-likelihood: replay of the recorded events */
 cudaError_t launch_grad_replay(const TransportParams& P, const DeviceTables& T, const uint32_t* events,

@@ -97,6 +97,8 @@ struct TransportParams {
   int sino_dry;           /* 1: detector draws as usual but no sinogram, image, spectrum writes */
   int dose_roi[6];        /* voxel dose ROI x0,x1,y0,y1,z0,z1 (0-based, clamped); x1 < 0: off */
   int quorum_rayleigh;    /* event loop: Rayleigh lanes needed to join a round with Compton lanes */
+  int max_steps;          /* Woodcock steps per photon before the guard drops it */
+  int max_rejections;     /* iterations per sampler rejection loop before the guard drops the photon */
 };
 
 /* Device pointers of one scene (all read-only during transport). */

@@ -81,6 +81,7 @@ struct mcpet_scene {
     float* activity = nullptr;
     unsigned long long* gwords = nullptr;  /* 0 replayed, 1 mismatches, 2 log-likelihood (double) */
     unsigned long long last_guard = 0;
+    bool last_run_noalloc = false;   /* mcpet_last_run_guard reads the allocation-free scratch */
     /* asynchronous host-buffer runs (mcpet_run_async): a second set of
      * tallies, snapshots of the run words, a download stream and events */
     int* trues_b = nullptr;

@@ -116,6 +116,8 @@ class RunOpts(C.Structure):
         ("seed_override", C.c_int),
         ("stream", C.c_void_p),
         ("algorithm", C.c_int),
+        ("max_woodcock_steps", C.c_int),
+        ("max_rejections", C.c_int),
     ]
 
 

@@ -281,6 +281,28 @@ def scanner_for_head() -> dict:
                 n_radial=256, n_z_slices=127, max_ring_difference=63, span=1)
 
 
+HEAD_WORKLOAD_SEED = 2024
+
+
+def head_workload(total_bq: float = 1.0e9, scanner: str = "head"):
+    """The head workload: 128x128x64 voxels of 2 mm (seed 2024), FDG-like
+    activity summing to total_bq, seen by the 64-ring scanner (256 x 256 x
+    8065 span-1 sinograms) with RANECU seed 12345.  scanner="head32" keeps the
+    phantom and ring pitch with 32 rings and 128 x 256 x 1985 sinograms (a
+    smaller case for profiler captures).  Returns (material, density,
+    activity, voxel_size, tissues, scanner keywords of spec_for)."""
+    mat, rho, act, vs, used = head_phantom(shape=(64, 128, 128), voxel_cm=0.2, seed=HEAD_WORKLOAD_SEED,
+                                           total_bq=total_bq)
+    scan = scanner_for_head()
+    if scanner == "head32":
+        scan.update(n_rows=32, n_z_slices=63, max_ring_difference=31, n_radial=128, n_angles=256, n_crystals=512,
+                    fov_z=12.8, detector_height=12.8)
+    elif scanner != "head":
+        raise ValueError(scanner)
+    scan["seed"] = 12345
+    return mat, rho, act, vs, used, scan
+
+
 def scanner_batch() -> dict:
     """41 cm radius, 32 rings x 4 mm, 128x128 sinograms (256 crystals), span 1,
     MRD 31: the scanner of the batched many-phantom workload."""

@@ -37,6 +37,8 @@ class RunOptions:
     seed_override: int = 0
     stream: int = 0
     algorithm: int = _abi.ALGORITHM_AUTO
+    max_woodcock_steps: int = 0     # device loop guards (<= 0: defaults 2^20 / 2^16)
+    max_rejections: int = 0
 
     def to_c(self) -> _abi.RunOpts:
         o = _abi.RunOpts()
@@ -49,6 +51,8 @@ class RunOptions:
         o.seed_override = int(self.seed_override)
         o.stream = self.stream or None
         o.algorithm = int(self.algorithm)
+        o.max_woodcock_steps = int(self.max_woodcock_steps)
+        o.max_rejections = int(self.max_rejections)
         return o
 
 

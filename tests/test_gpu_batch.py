@@ -138,8 +138,7 @@ def test_batch_rejects_invalid(tmp_path):
     other.close()
 
 
-needs_ref_prog = pytest.mark.skipif(not __import__("refbind").available("libref_prog.so"),
-                                    reason="reference CUDA build missing")
+needs_ref_prog = pytest.mark.needs_ref("libref_prog.so")
 
 
 @needs_ref_prog

@@ -19,7 +19,7 @@ import refbind
 import scenes
 
 pytestmark = pytest.mark.gpu
-needs_ref_prog = pytest.mark.skipif(not refbind.available("libref_prog.so"), reason="reference CUDA build missing")
+needs_ref_prog = pytest.mark.needs_ref("libref_prog.so")
 ROI = (2, 40, 3, 60, 5, 28)                    # 1-based, inside a 32x64x64 head
 
 

@@ -180,8 +180,7 @@ def test_autograd_binding(tmp_path):
     sc.close()
 
 
-needs_ref_prog = pytest.mark.skipif(not __import__("refbind").available("libref_prog.so"),
-                                    reason="reference CUDA build missing")
+needs_ref_prog = pytest.mark.needs_ref("libref_prog.so")
 
 
 @needs_ref_prog

@@ -22,7 +22,7 @@ import refbind
 import scenes
 from test_gpu_transport import assert_replay, replay
 
-needs_ref_prog = pytest.mark.skipif(not refbind.available("libref_prog.so"), reason="reference CUDA build missing")
+needs_ref_prog = pytest.mark.needs_ref("libref_prog.so")
 
 pytestmark = pytest.mark.gpu
 LONG_AXIAL = dict(detector_radius=-39.0, detector_height=102.4, fov_z=102.4, n_rows=256, n_crystals=768,

@@ -14,7 +14,7 @@ import scenes
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-needs_ref_gpu = pytest.mark.skipif(not refbind.available("libref_cuda.so"), reason="reference CUDA build missing")
+needs_ref_gpu = pytest.mark.needs_ref("libref_cuda.so")
 
 
 def _u8(a):

@@ -20,7 +20,7 @@ import refbind
 import scenes
 
 pytestmark = pytest.mark.gpu
-needs_ref_prog = pytest.mark.skipif(not refbind.available("libref_prog.so"), reason="reference CUDA build missing")
+needs_ref_prog = pytest.mark.needs_ref("libref_prog.so")
 
 
 def overlap(a: np.ndarray, b: np.ndarray) -> float:
