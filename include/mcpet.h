@@ -93,6 +93,19 @@ typedef struct {
   /* [SECTION VOXELIZED GEOMETRY FILE v.2009-11-30] / [SECTION MATERIAL FILE LIST] */
   char voxel_file[250];
   char material_files[MCPET_MAX_MATERIALS][250];
+  /* Optional [SECTION PROMPT GAMMA EMISSION v.2026-12-01], placed before the
+   * voxel-file section (the reference skips it while it looks for that
+   * section, MCGPU-PET.cu:1190-1202): an isotope that also emits a prompt
+   * gamma of this energy (eV) with this yield per decay (0 < yield <= 1),
+   * e.g. 1157020 eV at 1.0 for 44Sc.  The gamma leaves the decay point
+   * isotropically after the annihilation pair; every pair it forms with a
+   * detected annihilation photon is a candidate coincidence (spurious,
+   * tallied with the scatter).  No counterpart in the reference, which emits
+   * only 511 keV photons (MCGPU-PET_kernel.cu:669).  0 = no prompt gamma.
+   * Needs material tables that reach above the gamma energy and the
+   * sinogram tally only. */
+  float prompt_gamma_energy;
+  float prompt_gamma_yield;
 } mcpet_config;
 
 typedef struct mcpet_scene mcpet_scene;   /* opaque: phantom + tables + device copy */

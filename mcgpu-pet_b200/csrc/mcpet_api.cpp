@@ -148,6 +148,25 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.quorum_rayleigh = env_int("MCPET_QUORUM_RAYLEIGH", 2, 1, 32);
   P.max_steps = kMaxStepsDefault;
   P.max_rejections = kMaxRejectionsDefault;
+  P.prompt_energy = c.prompt_gamma_energy > 0.0f ? c.prompt_gamma_energy : 0.0f;
+  P.prompt_yield = c.prompt_gamma_energy > 0.0f ? c.prompt_gamma_yield : 0.0f;
+}
+
+/* A prompt-gamma scene needs the sinogram tally only and tables that reach
+ * above the gamma energy (its energy bin and the next one are read). */
+mcpet_status check_prompt(const mcpet_scene* sc) {
+  const mcpet_config& c = sc->cfg;
+  if (!(c.prompt_gamma_energy > 0.0f)) return MCPET_OK;
+  if (c.tally_psf_sinogram != 2)
+    return set_error(MCPET_ERR_ARG, "the prompt-gamma emitter supports the sinogram tally only (REPORT PSF/SINOGRAM 2)");
+  if (!(c.prompt_gamma_yield > 0.0f && c.prompt_gamma_yield <= 1.0f))
+    return set_error(MCPET_ERR_ARG, "prompt gamma yield %g outside (0, 1]", c.prompt_gamma_yield);
+  const double top = (double)sc->e0 + (double)(sc->n_e - 2) / (double)sc->ide;
+  if (!((double)c.prompt_gamma_energy < top))
+    return set_error(MCPET_ERR_ARG,
+                     "prompt gamma of %.0f eV above the material tables (last energy bin starts at %.0f eV): "
+                     "use tables that reach above it", (double)c.prompt_gamma_energy, top);
+  return MCPET_OK;
 }
 
 /* loop caps of a run: the options' values, or the defaults */
@@ -406,6 +425,10 @@ int auto_hpl_of(const std::vector<const mcpet_scene*>& scenes) {
 int auto_hpl(const mcpet_scene* sc) { return auto_hpl_of(std::vector<const mcpet_scene*>(1, sc)); }
 
 mcpet_status validate_opts(const mcpet_scene* sc, const mcpet_run_opts* opts) {
+  {
+    const mcpet_status ps = check_prompt(sc);
+    if (ps != MCPET_OK) return ps;
+  }
   int seed = (opts && opts->seed_override != 0) ? opts->seed_override : sc->cfg.seed;
   if (seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", seed);
   if (opts && (opts->lane_mode < 0 || opts->lane_mode > 1))
@@ -419,6 +442,10 @@ mcpet_status validate_opts(const mcpet_scene* sc, const mcpet_run_opts* opts) {
  * the zeroing of the outputs and the launch.  O.coincidences defaults to a
  * scene word. */
 mcpet_status prepare_params(mcpet_scene* sc, const mcpet_run_opts& o, DeviceTallies& O, TransportParams& P) {
+  {
+    const mcpet_status ps = check_prompt(sc);
+    if (ps != MCPET_OK) return ps;
+  }
   fill_params(sc, P);
   if (o.seed_override != 0) P.seed = o.seed_override;
   if (P.seed <= 0) return set_error(MCPET_ERR_ARG, "RANECU seed must be positive (got %d)", P.seed);
@@ -507,6 +534,18 @@ mcpet_status enqueue_run(mcpet_scene* sc, const mcpet_run_opts* opts, DeviceTall
   return launch_planned(sc, o, P, O, st, ms_out);
 }
 
+/* Kernel variant of a run: balanced lanes use the single-precision
+ * rotation and decay clock (they are held to statistical parity; reference
+ * lanes keep the reference's arithmetic for replay), prompt-gamma scenes the
+ * emitter, lowered caps the run-time loop guards. */
+int run_mode(const mcpet_scene* sc, const mcpet_run_opts& o) {
+  int m = 0;
+  if (o.lane_mode == MCPET_LANES_BALANCED) m |= kTransportFast;
+  if (sc->cfg.prompt_gamma_energy > 0.0f) m |= kTransportPrompt;
+  if (o.max_woodcock_steps > 0 || o.max_rejections > 0) m |= kTransportCaps;
+  return m;
+}
+
 /* Launch the transport for a prepared run (P, O complete, the work-queue
  * word set), optionally timed. */
 mcpet_status launch_planned(mcpet_scene* sc, const mcpet_run_opts& o, TransportParams& P, DeviceTallies& O,
@@ -514,20 +553,29 @@ mcpet_status launch_planned(mcpet_scene* sc, const mcpet_run_opts& o, TransportP
   auto& d = sc->dev;
   const bool counters = o.collect_counters && O.counters;
   const int block = pick_block(o);
+  const int mode = run_mode(sc, o);
   int algorithm = o.algorithm == kAlgorithmHistories ? kAlgorithmHistories : kAlgorithmEvents;
-  if (algorithm == kAlgorithmEvents && env_int("MCPET_MINBLOCKS", 4, 1, 4) == 1) algorithm = kAlgorithmEventsUncapped;
+  if (algorithm == kAlgorithmEvents && env_int("MCPET_MINBLOCKS", 4, 1, 4) == 1 && (mode & ~kTransportFast) == 0)
+    algorithm = kAlgorithmEventsUncapped;
   if (O.events && algorithm != kAlgorithmHistories) algorithm = kAlgorithmEventsRecord;
   else if ((O.mat_dose || O.vox_dose) && algorithm != kAlgorithmHistories) algorithm = kAlgorithmEventsDose;
+  /* lowered loop caps: the plain event kernel and the history loop read them
+   * (the history loop also when the run tallies dose or a prompt gamma) */
+  if (mode & kTransportCaps) {
+    if (algorithm == kAlgorithmEventsRecord)
+      return set_error(MCPET_ERR_ARG, "lowered loop caps are not available for the gradient's recording run");
+    if (algorithm != kAlgorithmEvents || (mode & kTransportPrompt)) algorithm = kAlgorithmHistories;
+  }
   size_t smem = transport_dynamic_smem(P, block, algorithm);
   int bps = 0;
-  CUDA_TRY(transport_occupancy(counters, algorithm, block, smem, &bps));
+  CUDA_TRY(transport_occupancy(counters, algorithm, mode, block, smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   int grid = d.sm_count * bps;
   d.last_h2d = d.run_h2d + (long long)sizeof(TransportParams);
   if (P.n_lanes == 0) grid = 1;
   if (ms_out) CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev0, st));
-  CUDA_TRY(launch_transport(P, device_tables(sc), O, counters, algorithm, grid, block, smem, st));
+  CUDA_TRY(launch_transport(P, device_tables(sc), O, counters, algorithm, mode, grid, block, smem, st));
   if (ms_out) {
     CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
     CUDA_TRY(cudaEventSynchronize((cudaEvent_t)d.ev1));
@@ -758,6 +806,7 @@ struct BatchLaunch {
   uint64_t total = 0;
   bool counters = false, dose = false;
   int share = 0;                    /* kBatchShareScanner | kBatchSharePhantom */
+  int mode = 0;                     /* kernel variant (fast arithmetic, prompt gamma) */
   int grid = 1, block = 0;
   size_t smem = 0;
   /* device blob: slots | Compton table | Rayleigh float rows | Rayleigh byte rows */
@@ -866,6 +915,9 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   L.P.n_lanes = L.total;
   L.P.n_emitters = 0;
   L.P.max_shells = max_shells;
+  /* the launch's shared layout holds the prompt-gamma fields when any scene
+   * emits one (each lane reads its own scene's emitter) */
+  for (const SceneSlot& z : L.slots) L.P.prompt_energy = std::max(L.P.prompt_energy, z.P.prompt_energy);
   L.T = L.slots[0].T;
   L.T.emitters = nullptr;
   L.counters = o.collect_counters && outs[0].counters;
@@ -893,7 +945,11 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
       L.smem = transport_batch_dynamic_smem(L.P, L.block);
     }
   }
-  CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.share, L.block, L.smem, &bps));
+  if (o.max_woodcock_steps > 0 || o.max_rejections > 0)
+    return set_error(MCPET_ERR_ARG, "lowered loop caps are available for single-scene runs only");
+  L.mode = (o.lane_mode == MCPET_LANES_BALANCED ? kTransportFast : 0) |
+           (L.P.prompt_energy > 0.0f ? kTransportPrompt : 0);
+  CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.share, L.mode, L.block, L.smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", L.smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   L.grid = L.total == 0 ? 1 : s0->dev.sm_count * bps;
@@ -945,7 +1001,7 @@ mcpet_status enqueue_batch_launch(mcpet_scene* const* scenes, int n, BatchLaunch
   }
   if (ev0) CUDA_TRY(cudaEventRecord(ev0, st));
   CUDA_TRY(launch_transport_batch(L.P, L.T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, L.counters, L.dose,
-                                  L.share, L.grid, L.block, L.smem, st));
+                                  L.share, L.mode, L.grid, L.block, L.smem, st));
   if (ev1) CUDA_TRY(cudaEventRecord(ev1, st));
   return MCPET_OK;
 }
@@ -1713,6 +1769,8 @@ mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_talli
     return set_error(MCPET_ERR_ARG, "the gradient needs the trues and scatter sinograms of the forward run");
   if (!(sc->cfg.tally_psf_sinogram == 0 || sc->cfg.tally_psf_sinogram == 2))
     return set_error(MCPET_ERR_ARG, "the gradient needs the sinogram tally (REPORT PSF/SINOGRAM 0 or 2)");
+  if (sc->cfg.prompt_gamma_energy > 0.0f)
+    return set_error(MCPET_ERR_ARG, "the gradient replays annihilation pairs only: no prompt-gamma emitter");
   if (g->event_buffer && g->event_capacity <= 0) return set_error(MCPET_ERR_ARG, "event_capacity must be > 0");
   mcpet_status s = validate_opts(sc, opts);
   if (s != MCPET_OK) return s;
@@ -1784,7 +1842,8 @@ mcpet_status mcpet_grad(mcpet_scene* sc, const mcpet_run_opts* opts, mcpet_talli
   if (n_events > 0 && (g->grad_activity || g->grad_density_scale))
     CUDA_TRY(launch_grad_replay(P, T, g->event_buffer ? (const uint32_t*)g->event_buffer : d.events, n_events,
                                 g->measured, device_out->trues, device_out->scatter, g->background, d.activity,
-                                g->grad_activity, g->grad_density_scale, d.gwords, d.sm_count, st));
+                                g->grad_activity, g->grad_density_scale, d.gwords, d.sm_count,
+                                (opts && opts->lane_mode == MCPET_LANES_BALANCED) ? kTransportFast : 0, st));
   CUDA_TRY(cudaEventRecord((cudaEvent_t)d.ev1, st));
   unsigned long long words[4];
   CUDA_TRY(cudaMemcpyAsync(words, d.gwords, sizeof(words), cudaMemcpyDeviceToHost, st));
@@ -1972,6 +2031,8 @@ mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_dev
     return set_error(MCPET_ERR_ARG, "sinogram tally requested but a sinogram/image/spectrum buffer is missing");
   if (!out->total_histories || !out->psf_count) return set_error(MCPET_ERR_ARG, "histories and psf_count are required");
 
+  s = check_prompt(sc);
+  if (s != MCPET_OK) return s;
   TransportParams P;
   fill_params(sc, P);
   if (o.seed_override != 0) P.seed = o.seed_override;
@@ -2009,16 +2070,19 @@ mcpet_status mcpet_run_device_noalloc(mcpet_scene* sc, const float* activity_dev
   const bool counters = o.collect_counters && O.counters;
   if (O.counters) CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
 
+  if (o.max_woodcock_steps > 0 || o.max_rejections > 0)
+    return set_error(MCPET_ERR_ARG, "lowered loop caps are not available for the allocation-free run");
+  const int mode = run_mode(sc, o);
   int block = transport_block_threads();
   size_t smem = transport_dynamic_smem(P, block, kAlgorithmEvents);
   int bps = 0;
-  CUDA_TRY(transport_occupancy(counters, kAlgorithmEvents, block, smem, &bps));
+  CUDA_TRY(transport_occupancy(counters, kAlgorithmEvents, mode, block, smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   const int grid = d.sm_count * bps;
   d.last_run_noalloc = true;
   CUDA_TRY(launch_transport_noalloc(P, device_tables(sc), O, activity_device, o.lane_mode, tpb, hpl, d.sm_count,
-                                    counters, grid, block, smem, st));
+                                    counters, mode, grid, block, smem, st));
   return MCPET_OK;
 }
 

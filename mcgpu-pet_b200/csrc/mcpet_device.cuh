@@ -199,6 +199,58 @@ __device__ __forceinline__ void rotate(float3& d, double costh, double phi) {
   }
 }
 
+/* The same direction change in single precision, for balanced lanes (which
+ * are held to statistical parity, not history replay): azimuth phi = 2 pi u
+ * from the same random draw, the new direction from the same formulas.  The
+ * double-precision sincos, square roots and divisions of the reference form
+ * are the most expensive arithmetic of a scattering round on this part. */
+__device__ __forceinline__ void rotate_fast(float3& d, float costh, float u) {
+  float sinphi, cosphi;
+  __sincosf(6.28318530717958647693f * u, &sinphi, &cosphi);
+  float dxy = d.x * d.x + d.y * d.y;
+  const float norm = dxy + d.z * d.z;
+  if (fabsf(norm - 1.0f) > 1.0e-6f) {
+    const float s = rsqrtf(norm);
+    d.x *= s;
+    d.y *= s;
+    d.z *= s;
+    dxy = d.x * d.x + d.y * d.y;
+  }
+  if (dxy > 1.0e-14f) {
+    const float sdt = sqrtf((1.0f - costh * costh) / dxy);
+    const float x_in = d.x;
+    d.x = d.x * costh + sdt * (x_in * d.z * cosphi - d.y * sinphi);
+    d.y = d.y * costh + sdt * (d.y * d.z * cosphi + x_in * sinphi);
+    d.z = d.z * costh - dxy * sdt * cosphi;
+  } else {
+    const float sdt = sqrtf(1.0f - costh * costh);
+    d.y = sdt * sinphi;
+    if (d.z > 0.0f) {
+      d.x = sdt * cosphi;
+      d.z = costh;
+    } else {
+      d.x = -sdt * cosphi;
+      d.z = -costh;
+    }
+  }
+}
+
+/* Time to a lane's next decay in ps, and the lane's decayed 1/rate
+ * (MCGPU-PET_kernel.cu:267-291).  kFast: the exponential interval in single
+ * precision from the same draw (balanced lanes); otherwise the reference's
+ * double-precision form. */
+template <bool kFast>
+__device__ __forceinline__ unsigned long long decay_interval(Rng& r, double& inv_rate, double inv_mean_life) {
+  if (kFast) {
+    const float dt_ps = -__logf(ranecu(r)) * (float)(inv_rate * 1e12);
+    inv_rate = inv_rate * (double)__expf(dt_ps * (float)(inv_mean_life * 1e-12));
+    return __float2ull_rn(dt_ps);
+  }
+  const double dt = -log(ranecu_double(r)) * inv_rate;
+  inv_rate = inv_rate * exp(dt * inv_mean_life);
+  return __double2ull_rn(dt * 1e12);
+}
+
 /* ------------------------------------------------------------------------
  * Rayleigh scattering: RITA sampling of the squared molecular form factor
  * plus rejection (PENELOPE 2006 GRAa; MCGPU-PET_kernel.cu:1231-1296).

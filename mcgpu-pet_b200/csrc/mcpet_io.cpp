@@ -85,6 +85,17 @@ bool seek_section(LineReader& r, const char* key) {
   }
 }
 
+/* Skip lines until one holds key a (returns 1) or key b (returns 2); 0 at
+ * the end of the file. */
+int seek_either(LineReader& r, const char* a, const char* b) {
+  char line[kLine];
+  for (;;) {
+    if (!r.get(line)) return 0;
+    if (strstr(line, a) != nullptr) return 1;
+    if (strstr(line, b) != nullptr) return 2;
+  }
+}
+
 bool yes_answer(const char* s) {
   return strncmp("YE", s, 2) == 0 || strncmp("Ye", s, 2) == 0 || strncmp("ye", s, 2) == 0;
 }
@@ -251,8 +262,27 @@ mcpet_status parse_input(const char* in_path, mcpet_config* cfg) {
   if (cfg->span <= 0) return set_error(MCPET_ERR_FORMAT, "SPAN must be positive (got %d)", cfg->span);
   derive_sinogram_sizes(cfg);
 
-  if (!seek_section(r, "SECTION VOXELIZED GEOMETRY FILE v.2009-11-30"))
+  /* optional prompt-gamma section before the voxel-file section */
+  cfg->prompt_gamma_energy = 0.0f;
+  cfg->prompt_gamma_yield = 0.0f;
+  const int found = seek_either(r, "SECTION PROMPT GAMMA EMISSION v.2026-12-01",
+                                "SECTION VOXELIZED GEOMETRY FILE v.2009-11-30");
+  if (found == 1) {
+    next_value_line(r, v);
+    if (sscanf(v, "%f", &cfg->prompt_gamma_energy) != 1)
+      return set_error(MCPET_ERR_FORMAT, "prompt gamma energy (eV) expected, got '%s'", v);
+    next_value_line(r, v);
+    if (sscanf(v, "%f", &cfg->prompt_gamma_yield) != 1)
+      return set_error(MCPET_ERR_FORMAT, "prompt gamma yield per decay expected, got '%s'", v);
+    if (!(cfg->prompt_gamma_energy >= 0.0f) || (cfg->prompt_gamma_energy > 0.0f &&
+                                                !(cfg->prompt_gamma_yield > 0.0f && cfg->prompt_gamma_yield <= 1.0f)))
+      return set_error(MCPET_ERR_FORMAT, "prompt gamma: energy %g eV must be >= 0 and the yield %g in (0, 1]",
+                       cfg->prompt_gamma_energy, cfg->prompt_gamma_yield);
+    if (!seek_section(r, "SECTION VOXELIZED GEOMETRY FILE v.2009-11-30"))
+      return set_error(MCPET_ERR_FORMAT, "input file lacks 'SECTION VOXELIZED GEOMETRY FILE v.2009-11-30'");
+  } else if (found != 2) {
     return set_error(MCPET_ERR_FORMAT, "input file lacks 'SECTION VOXELIZED GEOMETRY FILE v.2009-11-30'");
+  }
   next_value_line(r, v);
   first_word(v, cfg->voxel_file, sizeof(cfg->voxel_file));
 

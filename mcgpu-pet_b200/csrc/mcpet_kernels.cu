@@ -37,6 +37,28 @@ struct LaneCounters {
   unsigned long long steps, refresh, majorant, tallies, photons, compton, rayleigh, photo, lanes, guard;
 };
 
+/* Compile-time variants of the transport kernels (kMode bits): kModeFast
+ * is the single-precision direction rotation and decay clock of balanced
+ * lanes; kModePrompt compiles the prompt-gamma emitter; kModeCaps reads the
+ * loop guards' caps from the run parameters instead of the defaults.  A
+ * variant carries none of the code of the features it leaves out. */
+constexpr int kModeFast = kTransportFast, kModePrompt = kTransportPrompt, kModeCaps = kTransportCaps;
+
+template <int kMode>
+__device__ __forceinline__ int steps_cap(const TransportParams& P) {
+  return (kMode & kModeCaps) ? P.max_steps : kMaxWoodcockSteps;
+}
+template <int kMode>
+__device__ __forceinline__ int rejections_cap(const TransportParams& P) {
+  return (kMode & kModeCaps) ? P.max_rejections : kMaxRejections;
+}
+/* direction change after a real scattering with the next random draw */
+template <int kMode>
+__device__ __forceinline__ void scatter_direction(Rng& rng, float3& dir, double costh) {
+  if (kMode & kModeFast) rotate_fast(dir, (float)costh, ranecu(rng));
+  else rotate(dir, costh, 6.28318530717958647693 * ranecu_double(rng));
+}
+
 template <bool kCount>
 struct Counting;
 template <>
@@ -118,13 +140,17 @@ struct NoStepHook {
 /* Transport one photon from its emission point until it leaves the voxel box
  * (returns true) or is absorbed (returns false).  Woodcock delta tracking and
  * interaction selection of MCGPU-PET_kernel.cu:298-414. */
-template <bool kCount, typename Scratch, typename Hook = NoStepHook>
+template <bool kCount, int kMode, typename Scratch, typename Hook = NoStepHook>
 __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P, const DeviceTables& T,
                                              const PaletteEntry* pal, const ComptonTable& C, Scratch rn,
                                              PhotonState& ph, LaneCounters& cnt, Hook* hook = nullptr,
                                              const DoseSink* dose = nullptr) {
   float energy = ph.energy;
   int index = __float2int_rd((energy - P.e0) * P.ide);
+  if ((kMode & kModePrompt) && (index < 0 || index >= P.n_e - 1)) {   /* energy outside the tables */
+    Counting<true>::add(cnt.guard, 1);
+    return false;
+  }
   float2 w = __ldg(reinterpret_cast<const float2*>(T.woodcock) + index);
   float mfp_w = w.x + energy * w.y;
   Counting<kCount>::add(cnt.majorant, 1);
@@ -144,7 +170,7 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       ph.pos.z += step * ph.dir.z;
       vox = locate(P, ph.pos.x, ph.pos.y, ph.pos.z);
       if (vox < 0) break;
-      if ((unsigned long long)vox >= (unsigned long long)P.n_voxels || ++steps > P.max_steps) {
+      if ((unsigned long long)vox >= (unsigned long long)P.n_voxels || ++steps > steps_cap<kMode>(P)) {
         Counting<true>::add(cnt.guard, 1);
         ph.energy = energy;
         return false;
@@ -172,12 +198,12 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       /* Compton */
       double costh;
       const float e_before = energy;
-      if (!sample_compton(rng, energy, mat0, C, rn, costh, nullptr, P.max_rejections)) {
+      if (!sample_compton(rng, energy, mat0, C, rn, costh, nullptr, rejections_cap<kMode>(P))) {
         Counting<true>::add(cnt.guard, 1);
         ph.energy = energy;
         return false;
       }
-      rotate(ph.dir, costh, 6.28318530717958647693 * ranecu_double(rng));
+      scatter_direction<kMode>(rng, ph.dir, costh);
       Counting<kCount>::add(cnt.compton, 1);
       if (dose) (*dose)(P, energy - e_before, mat0, ph.pos);
       index = __float2int_rd((energy - P.e0) * P.ide);
@@ -193,12 +219,12 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       if (randno < prob) {
         /* Rayleigh */
         double costh;
-        if (!sample_rayleigh(rng, energy, mat0, rec_hi.z, T.rayleigh, costh, P.max_rejections)) {
+        if (!sample_rayleigh(rng, energy, mat0, rec_hi.z, T.rayleigh, costh, rejections_cap<kMode>(P))) {
           Counting<true>::add(cnt.guard, 1);
           ph.energy = energy;
           return false;
         }
-        rotate(ph.dir, costh, 6.28318530717958647693 * ranecu_double(rng));
+        scatter_direction<kMode>(rng, ph.dir, costh);
         ph.state = (ph.state == 0) ? 2 : 3;
         Counting<kCount>::add(cnt.rayleigh, 1);
       } else {
@@ -237,12 +263,15 @@ __device__ __forceinline__ void put_psf_record(uint32_t* psf, long long k, unsig
  * (MCGPU-PET_kernel.cu:417-432): sinogram tally (tally_Sinogram,
  * :1624-1836) and/or phase-space tally (tally_PSF_coincidences, :531-644).
  * "b" = the second photon (tracked last), "a" = the first.  `centre` is the
- * detector centre (P.cx, P.cy, P.cz). */
+ * detector centre (P.cx, P.cy, P.cz).  A spurious pair (a prompt gamma with
+ * an annihilation photon) is tallied with the scatter whatever the photons'
+ * scatter states. */
 template <bool kCount, bool kRecord = true>
 __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, const float3 centre,
                                             const DeviceTallies& O, int* spec_sh, int voxel,
                                             unsigned long long t_left, const PhotonState& b, const PhotonState& a,
-                                            LaneCounters& cnt, unsigned long long& detected, int2 rng_emit) {
+                                            LaneCounters& cnt, unsigned long long& detected, int2 rng_emit,
+                                            bool spurious = false) {
   const bool want_sino = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 2);
   const bool want_psf = (P.tally_psf_sinogram == 0) || (P.tally_psf_sinogram == 1);
   if (want_sino) {
@@ -274,7 +303,7 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
           }
           if (eb > P.e_low && eb < P.e_high && ea > P.e_low && ea < P.e_high && !P.sino_dry) {
             if (bin < P.nbins) {
-              if (b.state == 0 && a.state == 0) {
+              if (!spurious && b.state == 0 && a.state == 0) {
                 atomicAdd(&O.trues[bin], 1);
                 atomicAdd(&O.image_trues[voxel], 1);
               } else {
@@ -354,7 +383,7 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
 
 constexpr int kBlock = 256;
 
-template <bool kCount>
+template <bool kCount, int kMode>
 __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, DeviceTables T, DeviceTallies O) {
   __shared__ ComptonTable cmp;
   __shared__ unsigned long long mdose_sh[2 * kMaxMaterials];
@@ -408,12 +437,10 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
 
     for (;;) {
       /* time to the next decay of this lane (MCGPU-PET_kernel.cu:267-291) */
-      double dt = -log(ranecu_double(rng)) * inv_act;
-      unsigned long long dt_ps = __double2ull_rn(dt * 1e12);
+      const unsigned long long dt_ps = decay_interval<(kMode & kModeFast) != 0>(rng, inv_act, P.inv_mean_life);
       if (!(dt_ps < t_left)) break;
       t_left = t_left - dt_ps;
       histories += 2;
-      inv_act = inv_act * exp(dt * P.inv_mean_life);
 
       PhotonState a, b;
       const int2 rng_emit = make_int2(rng.x, rng.y);
@@ -423,14 +450,16 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       a.travel = 0.0f;
       a.state = 0;
       Counting<kCount>::add(cnt.photons, 2);
-      bool esc_a = track_photon<kCount>(rng, P, T, pal, cmp, rn, a, cnt, (NoStepHook*)nullptr, dose_on ? &dose : nullptr);
+      bool esc_a =
+          track_photon<kCount, kMode>(rng, P, T, pal, cmp, rn, a, cnt, (NoStepHook*)nullptr, dose_on ? &dose : nullptr);
 
       emit_second(rng, background, dir0, b.dir);
       b.pos = origin;
       b.energy = kAnnihilation;
       b.travel = 0.0f;
       b.state = 0;
-      bool esc_b = track_photon<kCount>(rng, P, T, pal, cmp, rn, b, cnt, (NoStepHook*)nullptr, dose_on ? &dose : nullptr);
+      bool esc_b =
+          track_photon<kCount, kMode>(rng, P, T, pal, cmp, rn, b, cnt, (NoStepHook*)nullptr, dose_on ? &dose : nullptr);
 
       if (esc_a && esc_b) {
         bool pass = (P.tally_type == 0) || (P.tally_type == 1 && b.state == 0 && a.state == 0) ||
@@ -438,6 +467,29 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
         if (pass)
           detect_pair<kCount>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel, t_left, b, a, cnt, detected,
                               rng_emit);
+      }
+      /* prompt gamma: isotropic from the decay point after the pair, then
+       * its pairs with the annihilation photons that escaped (spurious
+       * coincidences; not in the trues-only tally) */
+      if ((kMode & kModePrompt) && (P.prompt_yield >= 1.0f || ranecu(rng) < P.prompt_yield)) {
+        PhotonState g;
+        emit_isotropic(rng, g.dir);
+        g.pos = origin;
+        g.energy = P.prompt_energy;
+        g.travel = 0.0f;
+        g.state = 0;
+        histories += 1;
+        Counting<kCount>::add(cnt.photons, 1);
+        const bool esc_g = track_photon<kCount, kMode>(rng, P, T, pal, cmp, rn, g, cnt, (NoStepHook*)nullptr,
+                                                       dose_on ? &dose : nullptr);
+        if (esc_g && P.tally_type != 1) {
+          if (esc_a)
+            detect_pair<kCount>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel, t_left, g, a, cnt,
+                                detected, rng_emit, true);
+          if (esc_b)
+            detect_pair<kCount>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel, t_left, g, b, cnt,
+                                detected, rng_emit, true);
+        }
       }
     }
   }
@@ -491,6 +543,8 @@ enum : int {
   kCRx, kCRy,                                    /* RANECU state right before the pair's emission */
   kCHist, kCDet,                                 /* batch only: lane photons started, coincidences tallied */
   kCPmax,                                        /* batch only: Rayleigh pmax of the pending interaction */
+  kCBx, kCBy, kCBz, kCBu, kCBv, kCBw,            /* prompt gamma only: photon 2 at exit: position, direction, */
+  kCBe, kCBt, kCBs,                              /* energy (-10 absorbed), travel, state */
   kCold
 };
 constexpr int kColdSingle = kCHist;              /* fields a single-scene launch uses (the last ones need no room) */
@@ -525,7 +579,7 @@ constexpr int kShareScanner = kBatchShareScanner;
 constexpr int kSharePhantom = kBatchSharePhantom;
 
 template <bool kCount, int kMinBlocks = 1, bool kDevicePlan = false, bool kBatch = false, bool kRecord = false,
-          bool kDose = false, int kShare = 0>
+          bool kDose = false, int kShare = 0, int kMode = 0>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(TransportParams P, DeviceTables T,
                                                                               DeviceTallies O,
                                                                               const SceneSlot* __restrict__ slots,
@@ -629,11 +683,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   };
 
   /* (the scenes of a batch share the energy grid: e0 and ide are P's) */
-  auto start_photon = [&](const DeviceTables& TW) {
-    ph.energy = kAnnihilation;
+  auto start_photon = [&](const DeviceTables& TW, float energy) {
+    ph.energy = energy;
     ph.travel = 0.0f;
     ph.state = 0;
     index = __float2int_rd((ph.energy - P.e0) * P.ide);
+    Counting<kCount>::add(cnt.photons, 1);
+    if ((kMode & kModePrompt) && (index < 0 || index >= P.n_e - 1)) {   /* energy outside the tables */
+      Counting<true>::add(cnt.guard, 1);
+      escaped = false;
+      phase = kPhEnd;
+      return;
+    }
     float2 w = __ldg(reinterpret_cast<const float2*>(TW.woodcock) + index);
     mfp_w = w.x + ph.energy * w.y;
     mat_old = -1;
@@ -641,7 +702,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
     fresh = true;
     phase = kPhStep;
     Counting<kCount>::add(cnt.majorant, 1);
-    Counting<kCount>::add(cnt.photons, 1);
   };
 
   for (;;) {
@@ -677,9 +737,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
         bool ok;
         float e = ph.energy;
         if (is_compton) {
-          ok = sample_compton(rng, e, mat0, cmp, rn, costh, s0_ann, P.max_rejections);
+          ok = sample_compton(rng, e, mat0, cmp, rn, costh, s0_ann, rejections_cap<kMode>(P));
         } else {
-          ok = sample_rayleigh(rng, e, mat0, kBatch ? cold.f(kCPmax) : rec_hi.z, T.rayleigh, costh, P.max_rejections);
+          ok = sample_rayleigh(rng, e, mat0, kBatch ? cold.f(kCPmax) : rec_hi.z, T.rayleigh, costh,
+                               rejections_cap<kMode>(P));
         }
         if (!ok) {
           Counting<true>::add(cnt.guard, 1);
@@ -688,7 +749,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
         } else {
           const float e_before = ph.energy;
           ph.energy = e;
-          rotate(ph.dir, costh, 6.28318530717958647693 * ranecu_double(rng));
+          scatter_direction<kMode>(rng, ph.dir, costh);
           if (is_compton) {
             Counting<kCount>::add(cnt.compton, 1);
             if (dose_on) {
@@ -734,30 +795,61 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           emit_second(rng, background, d0, ph.dir);
           ph.pos = make_float3(cold.f(kCOx), cold.f(kCOy), cold.f(kCOz));
           which = 2;
-          start_photon(TG);
+          start_photon(TG, kAnnihilation);
         } else {
-          const float ea = cold.f(kCAe);
-          if (escaped && ea > -0.5f) {
-            PhotonState a;
-            a.pos = make_float3(cold.f(kCAx), cold.f(kCAy), cold.f(kCAz));
-            a.dir = make_float3(cold.f(kCAu), cold.f(kCAv), cold.f(kCAw));
-            a.energy = ea;
-            a.travel = cold.f(kCAt);
-            a.state = (int)cold.u(kCAs);
-            const bool pass = (PD.tally_type == 0) || (PD.tally_type == 1 && ph.state == 0 && a.state == 0) ||
-                              (PD.tally_type == 2 && (ph.state != 0 || a.state != 0));
-            if (pass) {
-              unsigned long long det = 0;
-              detect_pair<kCount, kRecord>(rng, PD, make_float3(PD.cx, PD.cy, PD.cz), kBatch ? slots[scene].O : O,
-                                           spec_sh, (int)cold.u(kCVox),
-                                           cold.t_left(), ph, a, cnt, det,
-                                           kRecord ? make_int2((int)cold.u(kCRx), (int)cold.u(kCRy))
-                                                   : make_int2(0, 0));
-              if (kBatch) cold.u(kCDet) += (uint32_t)det;
-              else detected += det;
+          /* end of photon 2: its pair with photon 1; end of a prompt gamma
+           * (which == 3): its pairs with photons 1 and 2, spurious */
+          const bool prompt = (kMode & kModePrompt) && PS.prompt_energy > 0.0f;
+          if (which == 2 && prompt) {
+            if (escaped) {
+              cold.setf(kCBx, ph.pos.x); cold.setf(kCBy, ph.pos.y); cold.setf(kCBz, ph.pos.z);
+              cold.setf(kCBu, ph.dir.x); cold.setf(kCBv, ph.dir.y); cold.setf(kCBw, ph.dir.z);
+              cold.setf(kCBe, ph.energy); cold.setf(kCBt, ph.travel);
+              cold.u(kCBs) = (uint32_t)ph.state;
+            } else {
+              cold.setf(kCBe, -10.0f);
             }
           }
-          phase = kPhDecay;
+          const bool spurious = (kMode & kModePrompt) && which == 3;
+          const int partners = spurious ? 2 : 1;
+#pragma unroll 1
+          for (int k = 0; k < partners; ++k) {
+            const int f = k == 0 ? kCAx : kCBx;   /* photon 1 or photon 2: 9 fields in the same order */
+            const float ea = cold.f(f + (kCAe - kCAx));
+            if (escaped && ea > -0.5f) {
+              PhotonState a;
+              a.pos = make_float3(cold.f(f), cold.f(f + 1), cold.f(f + 2));
+              a.dir = make_float3(cold.f(f + 3), cold.f(f + 4), cold.f(f + 5));
+              a.energy = ea;
+              a.travel = cold.f(f + (kCAt - kCAx));
+              a.state = (int)cold.u(f + (kCAs - kCAx));
+              const bool pass = spurious ? (PD.tally_type != 1)
+                                         : (PD.tally_type == 0) || (PD.tally_type == 1 && ph.state == 0 && a.state == 0) ||
+                                               (PD.tally_type == 2 && (ph.state != 0 || a.state != 0));
+              if (pass) {
+                unsigned long long det = 0;
+                detect_pair<kCount, kRecord>(rng, PD, make_float3(PD.cx, PD.cy, PD.cz), kBatch ? slots[scene].O : O,
+                                             spec_sh, (int)cold.u(kCVox),
+                                             cold.t_left(), ph, a, cnt, det,
+                                             kRecord ? make_int2((int)cold.u(kCRx), (int)cold.u(kCRy))
+                                                     : make_int2(0, 0),
+                                             spurious);
+                if (kBatch) cold.u(kCDet) += (uint32_t)det;
+                else detected += det;
+              }
+            }
+          }
+          if (which == 2 && prompt && (PS.prompt_yield >= 1.0f || ranecu(rng) < PS.prompt_yield)) {
+            /* the prompt gamma: isotropic from the decay point */
+            emit_isotropic(rng, ph.dir);
+            ph.pos = make_float3(cold.f(kCOx), cold.f(kCOy), cold.f(kCOz));
+            which = 3;
+            if (kBatch) cold.u(kCHist) += 1;
+            else histories += 1;
+            start_photon(TG, PS.prompt_energy);
+          } else {
+            phase = kPhDecay;
+          }
         }
       }
       /* ---- next decay of the lane, or the next lane (MCGPU-PET_kernel.cu:259-298) */
@@ -798,8 +890,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           const TransportParams& PN = kBatch ? slots[scene].P : P;
           double inv_act = cold.inv_rate();
           unsigned long long t_left = cold.t_left();
-          double dt = -log(ranecu_double(rng)) * inv_act;
-          unsigned long long dt_ps = __double2ull_rn(dt * 1e12);
+          const unsigned long long dt_ps = decay_interval<(kMode & kModeFast) != 0>(rng, inv_act, PN.inv_mean_life);
           if (!(dt_ps < t_left)) {
             lane_live = false;
             continue;
@@ -810,7 +901,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             if (cold.u(kCHist) >= 0x80000000u) flush_lane();   /* keep the 32-bit word from wrapping */
           }
           else histories += 2;
-          cold.set_inv_rate(inv_act * exp(dt * PN.inv_mean_life));
+          cold.set_inv_rate(inv_act);
           const int voxel = (int)cold.u(kCVox);
           if (kRecord) {
             cold.u(kCRx) = (uint32_t)rng.x;
@@ -820,7 +911,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           cold.setf(kCOx, ph.pos.x); cold.setf(kCOy, ph.pos.y); cold.setf(kCOz, ph.pos.z);
           cold.setf(kCDx, ph.dir.x); cold.setf(kCDy, ph.dir.y); cold.setf(kCDz, ph.dir.z);
           which = 1;
-          start_photon((kBatch && !(kShare & kSharePhantom)) ? slots[scene].T : T);
+          start_photon((kBatch && !(kShare & kSharePhantom)) ? slots[scene].T : T, kAnnihilation);
           break;
         }
       }
@@ -850,7 +941,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             if (vox < 0) {
               escaped = true;
               phase = kPhEnd;
-            } else if ((unsigned long long)vox >= (unsigned long long)PG.n_voxels || ++steps > P.max_steps) {
+            } else if ((unsigned long long)vox >= (unsigned long long)PG.n_voxels || ++steps > steps_cap<kMode>(P)) {
               Counting<true>::add(cnt.guard, 1);
               escaped = false;
               phase = kPhEnd;
@@ -1083,6 +1174,7 @@ struct ScoreList {
   }
 };
 
+template <int kMode>
 __global__ void __launch_bounds__(kBlock) grad_replay_kernel(TransportParams P, DeviceTables T, const uint32_t* events,
                                                              unsigned long long n_events, const float* y,
                                                              const int* trues, const int* scatter, const float* bg,
@@ -1120,13 +1212,13 @@ __global__ void __launch_bounds__(kBlock) grad_replay_kernel(TransportParams P, 
     a.energy = kAnnihilation;
     a.travel = 0.0f;
     a.state = 0;
-    const bool esc_a = track_photon<false>(rng, P, T, T.palette, cmp, rn, a, cnt, &h);
+    const bool esc_a = track_photon<false, kMode>(rng, P, T, T.palette, cmp, rn, a, cnt, &h);
     emit_second(rng, background, dir0, b.dir);
     b.pos = origin;
     b.energy = kAnnihilation;
     b.travel = 0.0f;
     b.state = 0;
-    const bool esc_b = track_photon<false>(rng, P, T, T.palette, cmp, rn, b, cnt, &h);
+    const bool esc_b = track_photon<false, kMode>(rng, P, T, T.palette, cmp, rn, b, cnt, &h);
     /* the replayed pair must land in the recorded bin (geometry of the
      * sinogram tally, MCGPU-PET_kernel.cu:1645-1791) */
     bool ok = esc_a && esc_b && !h.overflow;
@@ -1411,17 +1503,27 @@ __global__ void plan_fill_kernel(const float* act, int nvox, int mode, int tpb, 
 
 /* ---------------------------------------------------------- launchers */
 
-size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm) {
+/* Dynamic shared memory: spectrum, palette, shell scratch and the event
+ * loop's per-thread fields (a single scene uses the fields before kCHist, a
+ * batch those before kCBx, a prompt-gamma scene all of them). */
+static size_t dynamic_smem(const TransportParams& P, int block, int algorithm, bool batch) {
   size_t s = 0;
   if (P.spectrum_in_shared) s += ((size_t)P.ne * 4 + 15) / 16 * 16;
   if (P.palette_in_shared) s += ((size_t)P.palette_in_shared * sizeof(PaletteEntry) + 15) / 16 * 16;
   s += (size_t)(P.max_shells > 0 ? P.max_shells : 1) * block * sizeof(float);
-  if (algorithm != kAlgorithmHistories) s += (size_t)kColdSingle * block * sizeof(uint32_t);
+  if (algorithm != kAlgorithmHistories) {
+    const int fields = P.prompt_energy > 0.0f ? kCold : (batch ? kCBx : kColdSingle);
+    s += (size_t)fields * block * sizeof(uint32_t);
+  }
   return s;
 }
 
+size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm) {
+  return dynamic_smem(P, block, algorithm, false);
+}
+
 size_t transport_batch_dynamic_smem(const TransportParams& P, int block) {
-  return transport_dynamic_smem(P, block, kAlgorithmEvents) + (size_t)(kCold - kColdSingle) * block * sizeof(uint32_t);
+  return dynamic_smem(P, block, kAlgorithmEvents, true);
 }
 
 int transport_block_threads() { return kBlock; }
@@ -1461,113 +1563,119 @@ static cudaError_t occupancy_of(K kernel, int block, size_t smem, int* bps) {
  * than the lost warps); kAlgorithmEventsUncapped keeps the uncapped build. */
 constexpr int kEventBlocks = 4;
 
-cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t smem, int* blocks_per_sm) {
+using EventKernel = void (*)(TransportParams, DeviceTables, DeviceTallies, const SceneSlot*, int);
+using HistoryKernel = void (*)(TransportParams, DeviceTables, DeviceTallies);
+
+/* The compiled variants of one event-kernel configuration, by mode: every
+ * mode below kModes (the modes a configuration supports: 2 = fast only,
+ * 4 = fast and prompt, 6 = also the caps, without prompt). */
+template <bool C, int B, bool D, bool Bt, bool R, bool Do, int S, int kModes>
+static EventKernel event_variant(int mode) {
+  switch (mode) {
+    case 0: return transport_events_kernel<C, B, D, Bt, R, Do, S, 0>;
+    case kModeFast: return transport_events_kernel<C, B, D, Bt, R, Do, S, kModeFast>;
+    case kModePrompt:
+      if (kModes >= 4) return transport_events_kernel<C, B, D, Bt, R, Do, S, (kModes >= 4 ? kModePrompt : 0)>;
+      return nullptr;
+    case kModePrompt | kModeFast:
+      if (kModes >= 4)
+        return transport_events_kernel<C, B, D, Bt, R, Do, S, (kModes >= 4 ? kModePrompt | kModeFast : 0)>;
+      return nullptr;
+    case kModeCaps:
+      if (kModes >= 6) return transport_events_kernel<C, B, D, Bt, R, Do, S, (kModes >= 6 ? kModeCaps : 0)>;
+      return nullptr;
+    case kModeCaps | kModeFast:
+      if (kModes >= 6)
+        return transport_events_kernel<C, B, D, Bt, R, Do, S, (kModes >= 6 ? kModeCaps | kModeFast : 0)>;
+      return nullptr;
+    default: return nullptr;
+  }
+}
+
+/* Single-scene transport kernel of a run: algorithm, counters, mode. */
+static EventKernel single_event_kernel(bool counters, int algorithm, int mode) {
   if (algorithm == kAlgorithmEventsDose)
-    return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, false, false, true>, block, smem,
-                                   blocks_per_sm)
-                    : occupancy_of(transport_events_kernel<false, kEventBlocks, false, false, false, true>, block,
-                                   smem, blocks_per_sm);
+    return counters ? event_variant<true, kEventBlocks, false, false, false, true, 0, 4>(mode)
+                    : event_variant<false, kEventBlocks, false, false, false, true, 0, 4>(mode);
   if (algorithm == kAlgorithmEventsRecord)
-    return counters
-               ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, false, true>, block, smem, blocks_per_sm)
-               : occupancy_of(transport_events_kernel<false, kEventBlocks, false, false, true>, block, smem,
-                              blocks_per_sm);
-  if (algorithm == kAlgorithmEvents)
-    return counters ? occupancy_of(transport_events_kernel<true, kEventBlocks>, block, smem, blocks_per_sm)
-                    : occupancy_of(transport_events_kernel<false, kEventBlocks>, block, smem, blocks_per_sm);
+    return counters ? event_variant<true, kEventBlocks, false, false, true, false, 0, 2>(mode)
+                    : event_variant<false, kEventBlocks, false, false, true, false, 0, 2>(mode);
   if (algorithm == kAlgorithmEventsUncapped)
-    return counters ? occupancy_of(transport_events_kernel<true>, block, smem, blocks_per_sm)
-                    : occupancy_of(transport_events_kernel<false>, block, smem, blocks_per_sm);
-  return counters ? occupancy_of(transport_kernel<true>, block, smem, blocks_per_sm)
-                  : occupancy_of(transport_kernel<false>, block, smem, blocks_per_sm);
+    return counters ? event_variant<true, 1, false, false, false, false, 0, 2>(mode)
+                    : event_variant<false, 1, false, false, false, false, 0, 2>(mode);
+  return counters ? event_variant<true, kEventBlocks, false, false, false, false, 0, 6>(mode)
+                  : event_variant<false, kEventBlocks, false, false, false, false, 0, 6>(mode);
+}
+
+template <bool C>
+static HistoryKernel history_variant(int mode) {
+  switch (mode & 7) {
+    case 0: return transport_kernel<C, 0>;
+    case 1: return transport_kernel<C, 1>;
+    case 2: return transport_kernel<C, 2>;
+    case 3: return transport_kernel<C, 3>;
+    case 4: return transport_kernel<C, 4>;
+    case 5: return transport_kernel<C, 5>;
+    case 6: return transport_kernel<C, 6>;
+    default: return transport_kernel<C, 7>;
+  }
+}
+
+cudaError_t transport_occupancy(bool counters, int algorithm, int mode, int block, size_t smem, int* blocks_per_sm) {
+  if (algorithm == kAlgorithmHistories)
+    return occupancy_of(counters ? history_variant<true>(mode) : history_variant<false>(mode), block, smem,
+                        blocks_per_sm);
+  EventKernel k = single_event_kernel(counters, algorithm, mode);
+  if (!k) return cudaErrorNotSupported;
+  return occupancy_of(k, block, smem, blocks_per_sm);
 }
 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                             bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream) {
-  if (algorithm == kAlgorithmEventsDose) {
-    if (counters)
-      transport_events_kernel<true, kEventBlocks, false, false, false, true><<<grid, block, smem, stream>>>(P, T, O,
-                                                                                                         nullptr, 0);
-    else
-      transport_events_kernel<false, kEventBlocks, false, false, false, true><<<grid, block, smem, stream>>>(P, T, O,
-                                                                                                          nullptr, 0);
-  } else if (algorithm == kAlgorithmEventsRecord) {
-    if (counters)
-      transport_events_kernel<true, kEventBlocks, false, false, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
-    else
-      transport_events_kernel<false, kEventBlocks, false, false, true><<<grid, block, smem, stream>>>(P, T, O, nullptr,
-                                                                                                   0);
-  } else if (algorithm == kAlgorithmEvents) {
-    if (counters) transport_events_kernel<true, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
-    else transport_events_kernel<false, kEventBlocks><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
-  } else if (algorithm == kAlgorithmEventsUncapped) {
-    if (counters) transport_events_kernel<true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
-    else transport_events_kernel<false><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
-  } else {
-    if (counters) transport_kernel<true><<<grid, block, smem, stream>>>(P, T, O);
-    else transport_kernel<false><<<grid, block, smem, stream>>>(P, T, O);
+                             bool counters, int algorithm, int mode, int grid, int block, size_t smem,
+                             cudaStream_t stream) {
+  if (algorithm == kAlgorithmHistories) {
+    HistoryKernel k = counters ? history_variant<true>(mode) : history_variant<false>(mode);
+    k<<<grid, block, smem, stream>>>(P, T, O);
+    return cudaGetLastError();
   }
+  EventKernel k = single_event_kernel(counters, algorithm, mode);
+  if (!k) return cudaErrorNotSupported;
+  k<<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   return cudaGetLastError();
 }
 
-cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int block, size_t smem,
-                                      int* blocks_per_sm) {
+/* Batched transport kernel: counters, dose, shared scanner/phantom, mode
+ * (fast, prompt). */
+static EventKernel batch_event_kernel(bool counters, bool dose, int share, int mode) {
   if (dose)
-    return counters
-               ? occupancy_of(transport_events_kernel<true, kEventBlocks, false, true, false, true>, block, smem,
-                              blocks_per_sm)
-               : occupancy_of(transport_events_kernel<false, kEventBlocks, false, true, false, true>, block, smem,
-                              blocks_per_sm);
-  if (counters)
-    return occupancy_of(transport_events_kernel<true, kEventBlocks, false, true>, block, smem, blocks_per_sm);
+    return counters ? event_variant<true, kEventBlocks, false, true, false, true, 0, 4>(mode)
+                    : event_variant<false, kEventBlocks, false, true, false, true, 0, 4>(mode);
+  if (counters) return event_variant<true, kEventBlocks, false, true, false, false, 0, 4>(mode);
   switch (share) {
     case kShareScanner:
-      return occupancy_of(transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner>,
-                          block, smem, blocks_per_sm);
+      return event_variant<false, kEventBlocks, false, true, false, false, kShareScanner, 4>(mode);
     case kSharePhantom:
-      return occupancy_of(transport_events_kernel<false, kEventBlocks, false, true, false, false, kSharePhantom>,
-                          block, smem, blocks_per_sm);
+      return event_variant<false, kEventBlocks, false, true, false, false, kSharePhantom, 4>(mode);
     case kShareScanner | kSharePhantom:
-      return occupancy_of(
-          transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner | kSharePhantom>, block,
-          smem, blocks_per_sm);
+      return event_variant<false, kEventBlocks, false, true, false, false, kShareScanner | kSharePhantom, 4>(mode);
     default:
-      return occupancy_of(transport_events_kernel<false, kEventBlocks, false, true>, block, smem, blocks_per_sm);
+      return event_variant<false, kEventBlocks, false, true, false, false, 0, 4>(mode);
   }
 }
 
+cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int mode, int block, size_t smem,
+                                      int* blocks_per_sm) {
+  EventKernel k = batch_event_kernel(counters, dose, share, mode);
+  if (!k) return cudaErrorNotSupported;
+  return occupancy_of(k, block, smem, blocks_per_sm);
+}
+
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int grid,
-                                   int block, size_t smem, cudaStream_t stream) {
-  if (dose) {
-    if (counters)
-      transport_events_kernel<true, kEventBlocks, false, true, false, true><<<grid, block, smem, stream>>>(P, T, O, slots,
-                                                                                                         n_slots);
-    else
-      transport_events_kernel<false, kEventBlocks, false, true, false, true><<<grid, block, smem, stream>>>(P, T, O,
-                                                                                                          slots, n_slots);
-    return cudaGetLastError();
-  }
-  if (counters) {
-    transport_events_kernel<true, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
-    return cudaGetLastError();
-  }
-  switch (share) {
-    case kShareScanner:
-      transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner>
-          <<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
-      break;
-    case kSharePhantom:
-      transport_events_kernel<false, kEventBlocks, false, true, false, false, kSharePhantom>
-          <<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
-      break;
-    case kShareScanner | kSharePhantom:
-      transport_events_kernel<false, kEventBlocks, false, true, false, false, kShareScanner | kSharePhantom>
-          <<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
-      break;
-    default:
-      transport_events_kernel<false, kEventBlocks, false, true><<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
-  }
+                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int mode,
+                                   int grid, int block, size_t smem, cudaStream_t stream) {
+  EventKernel k = batch_event_kernel(counters, dose, share, mode);
+  if (!k) return cudaErrorNotSupported;
+  k<<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
   return cudaGetLastError();
 }
 
@@ -1612,7 +1720,11 @@ static cudaError_t noalloc_scratch(NoAllocScratch** out) {
 
 cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,
                                      const float* activity, int lane_mode, int tpb, int hpl, int sm_count,
-                                     bool counters, int grid, int block, size_t smem, cudaStream_t stream) {
+                                     bool counters, int mode, int grid, int block, size_t smem,
+                                     cudaStream_t stream) {
+  EventKernel k = counters ? event_variant<true, kEventBlocks, true, false, false, false, 0, 4>(mode)
+                           : event_variant<false, kEventBlocks, true, false, false, false, 0, 4>(mode);
+  if (!k) return cudaErrorNotSupported;
   NoAllocScratch* S = nullptr;
   cudaError_t e = noalloc_scratch(&S);
   if (e != cudaSuccess) return e;
@@ -1633,14 +1745,9 @@ cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, D
   O.guard = &S->header[kHdrGuard];
   O.plan_counts = &S->header[kHdrLanes];
   if (!O.coincidences) O.coincidences = &S->header[kHdrCoinc];
-  if (counters) {
-    e = occupancy_smem_attr(transport_events_kernel<true, kEventBlocks, true>, smem);
-    if (e == cudaSuccess) transport_events_kernel<true, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
-  } else {
-    e = occupancy_smem_attr(transport_events_kernel<false, kEventBlocks, true>, smem);
-    if (e == cudaSuccess) transport_events_kernel<false, kEventBlocks, true><<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
-  }
+  e = occupancy_smem_attr(k, smem);
   if (e != cudaSuccess) return e;
+  k<<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
   return cudaGetLastError();
 }
 
@@ -1656,17 +1763,19 @@ cudaError_t noalloc_guard_trips(unsigned long long* trips) {
 cudaError_t launch_grad_replay(const TransportParams& P, const DeviceTables& T, const uint32_t* events,
                                unsigned long long n_events, const float* y, const int* trues, const int* scatter,
                                const float* bg, const float* activity, float* grad_a, float* grad_s,
-                               unsigned long long* stats, int sm_count, cudaStream_t stream) {
+                               unsigned long long* stats, int sm_count, int mode, cudaStream_t stream) {
+  /* the replay recomputes histories with the forward run's arithmetic */
+  auto kernel = (mode & kModeFast) ? grad_replay_kernel<kModeFast> : grad_replay_kernel<0>;
   const size_t smem = (size_t)(P.max_shells > 0 ? P.max_shells : 1) * kBlock * sizeof(float);
-  cudaError_t e = occupancy_smem_attr(grad_replay_kernel, smem);
+  cudaError_t e = occupancy_smem_attr(kernel, smem);
   if (e != cudaSuccess) return e;
   int bps = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, grad_replay_kernel, kBlock, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, kBlock, smem);
   if (e != cudaSuccess) return e;
   if (bps < 1) bps = 1;
   unsigned long long need = (n_events + kBlock - 1) / kBlock;
   int grid = (int)std::min<unsigned long long>(need > 0 ? need : 1, (unsigned long long)sm_count * bps);
-  grad_replay_kernel<<<grid, kBlock, smem, stream>>>(P, T, events, n_events, y, trues, scatter, bg, activity, grad_a,
+  kernel<<<grid, kBlock, smem, stream>>>(P, T, events, n_events, y, trues, scatter, bg, activity, grad_a,
                                                      grad_s, stats);
   return cudaGetLastError();
 }

@@ -14,11 +14,19 @@ constexpr int kAlgorithmEventsUncapped = 3; /* same loop, registers not capped (
 constexpr int kAlgorithmEventsRecord = 4;   /* event loop that also records tallied coincidences (gradient) */
 constexpr int kAlgorithmEventsDose = 5;     /* event loop with the dose tallies */
 
+/* Transport variants (bits of `mode` in the launchers): single-precision
+ * direction rotation and decay clock (balanced lanes), the prompt-gamma
+ * emitter, loop caps read from the run parameters. */
+constexpr int kTransportFast = 1;
+constexpr int kTransportPrompt = 2;
+constexpr int kTransportCaps = 4;
+
 size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();
-cudaError_t transport_occupancy(bool counters, int algorithm, int block, size_t smem, int* blocks_per_sm);
+cudaError_t transport_occupancy(bool counters, int algorithm, int mode, int block, size_t smem, int* blocks_per_sm);
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                             bool counters, int algorithm, int grid, int block, size_t smem, cudaStream_t stream);
+                             bool counters, int algorithm, int mode, int grid, int block, size_t smem,
+                             cudaStream_t stream);
 
 /* batched runs: several scenes in one launch of the event kernel.  share:
  * bit 0 = every scene has the launch's scanner (detector, sinogram, tally
@@ -28,11 +36,11 @@ cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, co
 size_t transport_batch_dynamic_smem(const TransportParams& P, int block);
 constexpr int kBatchShareScanner = 1;
 constexpr int kBatchSharePhantom = 2;
-cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int block, size_t smem,
+cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int mode, int block, size_t smem,
                                       int* blocks_per_sm);
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
-                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int grid,
-                                   int block, size_t smem, cudaStream_t stream);
+                                   const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int mode,
+                                   int grid, int block, size_t smem, cudaStream_t stream);
 
 /* batched regeneration: advance every slot's RANECU seed by `step` within
  * [1, m1 - 1] (the next replay of a captured batch) */
@@ -42,7 +50,8 @@ cudaError_t launch_advance_seeds(SceneSlot* slots, int n_slots, int step, cudaSt
 constexpr int kNoAllocMaxVoxels = 1 << 20;
 cudaError_t launch_transport_noalloc(const TransportParams& P, DeviceTables T, DeviceTallies O,
                                      const float* activity, int lane_mode, int tpb, int hpl, int sm_count,
-                                     bool counters, int grid, int block, size_t smem, cudaStream_t stream);
+                                     bool counters, int mode, int grid, int block, size_t smem,
+                                     cudaStream_t stream);
 /* guard trips of the last allocation-free call on the current device */
 cudaError_t noalloc_guard_trips(unsigned long long* trips);
 
@@ -50,7 +59,7 @@ cudaError_t noalloc_guard_trips(unsigned long long* trips);
 cudaError_t launch_grad_replay(const TransportParams& P, const DeviceTables& T, const uint32_t* events,
                                unsigned long long n_events, const float* y, const int* trues, const int* scatter,
                                const float* bg, const float* activity, float* grad_a, float* grad_s,
-                               unsigned long long* stats, int sm_count, cudaStream_t stream);
+                               unsigned long long* stats, int sm_count, int mode, cudaStream_t stream);
 cudaError_t launch_loglik(long long nbins, const float* y, const int* trues, const int* scatter, const float* bg,
                           double* out, int sm_count, cudaStream_t stream);
 

@@ -99,6 +99,8 @@ struct TransportParams {
   int quorum_rayleigh;    /* event loop: Rayleigh lanes needed to join a round with Compton lanes */
   int max_steps;          /* Woodcock steps per photon before the guard drops it */
   int max_rejections;     /* iterations per sampler rejection loop before the guard drops the photon */
+  float prompt_energy;    /* prompt gamma per decay (eV), 0 = none */
+  float prompt_yield;     /* its probability per decay (1: no draw) */
 };
 
 /* Device pointers of one scene (all read-only during transport). */

@@ -76,6 +76,8 @@ class Config(C.Structure):
         ("n_bins", C.c_longlong),
         ("voxel_file", C.c_char * 250),
         ("material_files", (C.c_char * 250) * MAX_MATERIALS),
+        ("prompt_gamma_energy", C.c_float),
+        ("prompt_gamma_yield", C.c_float),
     ]
 
 

@@ -23,9 +23,11 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 MATERIAL_DIR = os.path.join(PKG_DIR, "data", "materials")
 
 
-def material_path(name: str) -> str:
-    """Path of a material table (``air`` / ``water``) staged by the build."""
-    p = os.path.join(MATERIAL_DIR, f"{name}_5-515keV.mcgpu.gz")
+def material_path(name: str, extended: bool = False) -> str:
+    """Path of a material table (``air`` / ``water``) staged by the build:
+    the reference's 5-515 keV table, or (extended=True) the same table
+    continued to 1250 keV by mcpet.tables (for prompt gammas)."""
+    p = os.path.join(MATERIAL_DIR, f"{name}_5-1250keV.mcgpu.gz" if extended else f"{name}_5-515keV.mcgpu.gz")
     if not os.path.exists(p):
         raise FileNotFoundError(f"{p} missing: run __graft_entry__.build() to stage the material tables")
     return p
@@ -67,6 +69,8 @@ class InputSpec:
     span: int = 1
     voxel_file: str = "phantom.vox"
     material_files: List[str] = field(default_factory=list)
+    prompt_gamma_energy: float = 0.0        # eV; > 0 adds the optional prompt-gamma section
+    prompt_gamma_yield: float = 1.0         # per decay
 
 
 def write_input(path: str, s: InputSpec) -> str:
@@ -117,6 +121,17 @@ def write_input(path: str, s: InputSpec) -> str:
         f"{s.max_ring_difference}    # MAXIMUM RING DIFFERENCE",
         f"{s.span}    # SPAN",
         "",
+    ]
+    if s.prompt_gamma_energy > 0:
+        # read by this library only: the reference skips it while it looks for
+        # the voxel-file section
+        lines += [
+            "#[SECTION PROMPT GAMMA EMISSION v.2026-12-01]",
+            f"{s.prompt_gamma_energy!r}     # PROMPT GAMMA ENERGY (eV)",
+            f"{s.prompt_gamma_yield!r}      # PROMPT GAMMA YIELD PER DECAY",
+            "",
+        ]
+    lines += [
         "#[SECTION VOXELIZED GEOMETRY FILE v.2009-11-30]",
         f"{s.voxel_file}      # VOXEL GEOMETRY FILE",
         "",
@@ -173,14 +188,15 @@ TISSUES = {   # name: (material slot, table, density g/cm^3)
 }
 
 
-def tissue_materials(names: Sequence[str]) -> List[str]:
-    """Material file list (slot order) for the given tissues."""
+def tissue_materials(names: Sequence[str], extended: bool = False) -> List[str]:
+    """Material file list (slot order) for the given tissues (extended:
+    tables reaching 1250 keV)."""
     slots = {}
     for n in names:
         slot, table, _ = TISSUES[n]
-        slots[slot] = material_path(table)
+        slots[slot] = material_path(table, extended)
     top = max(slots)
-    return [slots.get(i, material_path("water")) for i in range(1, top + 1)]
+    return [slots.get(i, material_path("water", extended)) for i in range(1, top + 1)]
 
 
 def sample_phantom():

@@ -436,7 +436,7 @@ static void put_record(unsigned char* rec, unsigned long long t_emit, float trav
  * space tally (tally_PSF_coincidences, :531-644) of a pair whose photons both
  * escaped; b = second photon, a = first. */
 static void detect(rng_t* s, const orc_params* p, orc_outputs* o, int voxel, unsigned long long t_left,
-                   const photon* b, const photon* a, counts* cnt) {
+                   const photon* b, const photon* a, counts* cnt, int spurious) {
   const int sino = p->tally_psf_sinogram == 0 || p->tally_psf_sinogram == 2;
   const int psf = p->tally_psf_sinogram == 0 || p->tally_psf_sinogram == 1;
   if (sino) {
@@ -465,7 +465,7 @@ static void detect(rng_t* s, const orc_params* p, orc_outputs* o, int voxel, uns
             cnt->c[3]++;
           }
           if (eb > p->e_low && eb < p->e_high && ea > p->e_low && ea < p->e_high) {
-            if (b->state == 0 && a->state == 0) {
+            if (!spurious && b->state == 0 && a->state == 0) {
               add_i32(&o->trues[bin], 1);
               add_i32(&o->image_trues[voxel], 1);
             } else {
@@ -512,6 +512,7 @@ static int track(rng_t* s, const orc_params* p, const orc_tables* t, const int32
                  photon* ph, counts* cnt, orc_outputs* o) {
   float energy = ph->energy;
   int index = fl((energy - p->e0) * p->ide);
+  if (index < 0 || index >= p->n_e - 1) return 0;   /* outside the tables (callers check the prompt energy) */
   float mfp_w = t->woodcock[2 * index] + energy * t->woodcock[2 * index + 1];
   cnt->c[2]++;
   int mat_old = -1, mat = 0;
@@ -611,7 +612,27 @@ static unsigned long long run_lane(const orc_params* p, const orc_tables* t, con
     if (esc_a && esc_b) {
       int pass = (p->tally_type == 0) || (p->tally_type == 1 && b.state == 0 && a.state == 0) ||
                  (p->tally_type == 2 && (b.state != 0 || a.state != 0));
-      if (pass) detect(&s, p, o, voxel, t_left, &b, &a, cnt);
+      if (pass) detect(&s, p, o, voxel, t_left, &b, &a, cnt, 0);
+    }
+    /* Prompt gamma (no reference counterpart): emitted isotropically from
+     * the decay point after the pair (a yield draw first when the yield is
+     * below 1), tracked, then paired with each escaped annihilation photon,
+     * photon 1 first; every such pair is a spurious coincidence, tallied with
+     * the scatter and left out of a trues-only tally. */
+    if (p->prompt_energy > 0.0f && (p->prompt_yield >= 1.0f || ranecu(&s) < p->prompt_yield)) {
+      photon g;
+      isotropic(&s, &g.dir);
+      g.pos = origin;
+      g.energy = p->prompt_energy;
+      g.travel = 0.f;
+      g.state = 0;
+      hist += 1;
+      cnt->c[4] += 1;
+      int esc_g = track(&s, p, t, mat0, rho, &g, cnt, o);
+      if (esc_g && p->tally_type != 1) {
+        if (esc_a) detect(&s, p, o, voxel, t_left, &g, &a, cnt, 1);
+        if (esc_b) detect(&s, p, o, voxel, t_left, &g, &b, cnt, 1);
+      }
     }
   }
   return hist;

@@ -35,6 +35,8 @@ typedef struct {
   long long nbins;
   int tpb, seed, background;
   int dose_roi[6];             /* voxel dose ROI x0,x1,y0,y1,z0,z1 (0-based); x1 < 0: off */
+  float prompt_energy;         /* prompt gamma per decay (eV), 0 = none (no reference counterpart) */
+  float prompt_yield;          /* its probability per decay (>= 1: no draw) */
 } orc_params;
 
 typedef struct {

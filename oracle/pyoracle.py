@@ -35,6 +35,7 @@ class Params(C.Structure):
         ("nbins", C.c_longlong),
         ("tpb", C.c_int), ("seed", C.c_int), ("background", C.c_int),
         ("dose_roi", C.c_int * 6),
+        ("prompt_energy", C.c_float), ("prompt_yield", C.c_float),
     ]
 
 
@@ -110,6 +111,8 @@ class OracleScene:
         roi = list(cfg.dose_roi) if cfg.tally_voxel_dose else [0, -1, 0, -1, 0, -1]
         for k in range(6):
             p.dose_roi[k] = int(roi[k])
+        if cfg.prompt_gamma_energy > 0:
+            p.prompt_energy, p.prompt_yield = cfg.prompt_gamma_energy, cfg.prompt_gamma_yield
         self.material_dose = bool(cfg.tally_material_dose)
         self.n_dose = int(info.n_dose_voxels)
         self.p = p

@@ -9,19 +9,22 @@ import mcpet
 from mcpet import inputs
 
 
-def write_case(workdir: str, name: str, mat, rho, act, vs, tissues=("air", "soft"), gz: bool = False, **spec_kw):
-    """Write a .vox + .in pair in workdir; returns the .in path."""
+def write_case(workdir: str, name: str, mat, rho, act, vs, tissues=("air", "soft"), gz: bool = False,
+               extended: bool = False, **spec_kw):
+    """Write a .vox + .in pair in workdir; returns the .in path.  extended:
+    material tables continued to 1250 keV."""
     vox = inputs.write_vox(os.path.join(workdir, f"{name}.vox" + (".gz" if gz else "")), mat, rho, act, vs)
     kw = dict(inputs.scanner_small())
     kw.update(spec_kw)
-    spec = inputs.spec_for(inputs.tissue_materials(list(tissues)), vox, **kw)
+    spec = inputs.spec_for(inputs.tissue_materials(list(tissues), extended), vox, **kw)
     return inputs.write_input(os.path.join(workdir, f"{name}.in"), spec)
 
 
-def scene_from_arrays(workdir: str, mat, rho, act, vs, tissues=("air", "soft"), **spec_kw) -> mcpet.Scene:
+def scene_from_arrays(workdir: str, mat, rho, act, vs, tissues=("air", "soft"), extended: bool = False,
+                      **spec_kw) -> mcpet.Scene:
     kw = dict(inputs.scanner_small())
     kw.update(spec_kw)
-    spec = inputs.spec_for(inputs.tissue_materials(list(tissues)), "unused.vox", **kw)
+    spec = inputs.spec_for(inputs.tissue_materials(list(tissues), extended), "unused.vox", **kw)
     cfg = inputs.config_from_spec(spec, workdir)
     return mcpet.Scene.from_arrays(cfg, mat, rho, act, vs)
 

@@ -23,6 +23,9 @@ def _cases():
     yield "density_factor", (m, r, a, v, ("air", "soft")), {"density_factor": 0.37}
     m, r, a, v, used = inputs.head_phantom(shape=(12, 24, 24), voxel_cm=1.0, seed=5, total_bq=1e4)
     yield "head_tissues", (m, r, a, v, tuple(used)), dict(inputs.scanner_for_head())
+    # tables continued to 1250 keV (mcpet.tables), read by both loaders
+    yield "extended_tables", (m, r, a, v, tuple(used)), dict(inputs.scanner_for_head(), extended=True,
+                                                             prompt_gamma_energy=1157020.0)
 
 
 @pytest.mark.parametrize("name,arrays,kw", list(_cases()), ids=[c[0] for c in _cases()])
@@ -30,7 +33,8 @@ def test_tables_bit_identical_to_reference_loader(workdir, name, arrays, kw):
     mat, rho, act, vs, tissues = arrays
     kw = dict(kw)
     gz = kw.pop("gz", False)
-    inp = scenes.write_case(workdir, f"tab_{name}", mat, rho, act, vs, tissues=tissues, gz=gz, **kw)
+    ext = kw.pop("extended", False)
+    inp = scenes.write_case(workdir, f"tab_{name}", mat, rho, act, vs, tissues=tissues, gz=gz, extended=ext, **kw)
     ref_cfg, ref_vox, ref_t = refbind.RefIO().load(inp)
     with mcpet.Scene.load(inp) as sc:
         t = sc.export_tables()

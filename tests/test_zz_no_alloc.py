@@ -170,7 +170,8 @@ def test_noalloc_stream_limit_trip_reaches_the_caller(tmp_path):
     says so: counters[9] and mcpet_last_run_guard report the trip.  A
     following call within the limit is clean again."""
     torch = pytest.importorskip("torch")
-    mat, rho, act, vs = inputs.water_cube_phantom(729 * 3.0e6)   # 2.19e9 decays: 1 decay per lane is too many
+    mat, rho, _, vs = inputs.water_cube_phantom(1.0)
+    act = np.full(mat.shape, 3.0e6, np.float32)   # 2.19e9 decays: one lane per decay needs more than 2^31 streams
     sc = scenes.scene_from_arrays(str(tmp_path), mat, rho, act, vs)
     sc.to_device(0)
     cfg, info = sc.config, sc.info
