@@ -66,7 +66,7 @@ def test_prompt_gamma_statistics_vs_oracle(workdir, lanes):
     assert sc.guard_trips() == 0
     ref = pyoracle.OracleScene(sc, seed=2002).run(n_threads=0)
     # three photons per decay, each decay once in both runs up to Poisson noise
-    d_m, d_r = res.total_histories / 3, ref["histories"] / 3
+    d_m, d_r = res.total_histories / 3, ref["total_histories"] / 3
     assert abs(d_m - d_r) <= 3 * math.sqrt(d_m + d_r) + 1
     for k in ("trues", "scatter"):
         a, b = int(getattr(res, k).sum()), int(ref[k].sum())
@@ -94,7 +94,7 @@ def test_prompt_gamma_partial_yield_vs_oracle(workdir):
         a, b = int(getattr(res, k).sum()), int(ref[k].sum())
         assert abs(a - b) <= 3 * math.sqrt(a + b) + 1, (k, a, b)
     # 2 photons per decay plus one per emitted gamma: about 2.5 per decay
-    assert abs(res.total_histories / ref["histories"] - 1) < 0.01
+    assert abs(res.total_histories / ref["total_histories"] - 1) < 0.01
     sc.close()
 
 
