@@ -483,9 +483,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--algorithm", default="auto", choices=["auto", "histories", "events"])
-    ap.add_argument("--batch-scenes", type=int, default=0,
+    ap.add_argument("--batch-scenes", type=int, default=32,
                     help="also time N phantoms of m^3 voxels (m in [32,192], 1e8 decays each) batched in one "
-                         "launch against the same runs one by one (reported under 'batch')")
+                         "launch against the same runs one by one (reported under 'batch'; 0: skip; one GPU only)")
     ap.add_argument("--batch-emissions", type=float, default=1.0e8, help="decays per phantom of --batch-scenes")
     ap.add_argument("--no-gradient", action="store_true", help="skip the gradient (mcpet_grad) measurement")
     ap.add_argument("--beds", type=int, default=0,
@@ -658,7 +658,7 @@ def main():
         gradient = measure_gradient(tmp)
 
     batch = None
-    if args.batch_scenes > 0 and rank == 0:
+    if args.batch_scenes > 0 and rank == 0 and world == 1:
         batch = measure_batch(args.batch_scenes, tmp, args.batch_emissions)
 
     beds = None

@@ -138,19 +138,33 @@ __device__ __forceinline__ void emit_first(Rng& r, const TransportParams& P, int
 
 /* Second photon: anti-parallel to the first, tilted by the acolinearity
  * angle theta = 2*0.21276 deg * N(0,1) (Box-Muller, cosine branch) around a
- * uniform azimuth; or isotropic in background mode. */
+ * uniform azimuth; or isotropic in background mode.  kFast (balanced lanes):
+ * the same draws and formulas in single precision instead of the
+ * reference's double-precision constants and products. */
+template <bool kFast = false>
 __device__ __forceinline__ void emit_second(Rng& r, bool background, const float3& d1, float3& d) {
   if (background) {
     emit_isotropic(r, d);
     return;
   }
-  float phi2 = (float)((double)atan2f(d1.y, d1.x) + kPi);
-  float theta2 = (float)(kPi - (double)acosf(d1.z));
-  float v1 = ranecu(r);
-  float v2 = ranecu(r);
-  float theta_nc = (float)((2.0 * 0.21276 * kPi / 180.0) * (double)sqrtf(-2.0f * logf(v2 + 1e-8f)) *
-                           (double)cosf((float)((2.0 * kPi) * (double)v1)));
-  float phi_nc = (float)((2.0 * kPi) * (double)ranecu(r));
+  float phi2, theta2, theta_nc, phi_nc;
+  if (kFast) {
+    phi2 = atan2f(d1.y, d1.x) + (float)kPi;
+    theta2 = (float)kPi - acosf(d1.z);
+    const float v1 = ranecu(r);
+    const float v2 = ranecu(r);
+    theta_nc = (float)(2.0 * 0.21276 * kPi / 180.0) * sqrtf(-2.0f * __logf(v2 + 1e-8f)) *
+               __cosf((float)(2.0 * kPi) * v1);
+    phi_nc = (float)(2.0 * kPi) * ranecu(r);
+  } else {
+    phi2 = (float)((double)atan2f(d1.y, d1.x) + kPi);
+    theta2 = (float)(kPi - (double)acosf(d1.z));
+    const float v1 = ranecu(r);
+    const float v2 = ranecu(r);
+    theta_nc = (float)((2.0 * 0.21276 * kPi / 180.0) * (double)sqrtf(-2.0f * logf(v2 + 1e-8f)) *
+                       (double)cosf((float)((2.0 * kPi) * (double)v1)));
+    phi_nc = (float)((2.0 * kPi) * (double)ranecu(r));
+  }
   float st, ct, sp, cp, st1, ct1, sp1, cp1;
   sincosf(theta_nc, &st, &ct);
   sincosf(phi_nc, &sp, &cp);

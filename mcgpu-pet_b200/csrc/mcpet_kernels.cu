@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
       bool esc_a =
           track_photon<kCount, kMode>(rng, P, T, pal, cmp, rn, a, cnt, (NoStepHook*)nullptr, dose_on ? &dose : nullptr);
 
-      emit_second(rng, background, dir0, b.dir);
+      emit_second<(kMode & kModeFast) != 0>(rng, background, dir0, b.dir);
       b.pos = origin;
       b.energy = kAnnihilation;
       b.travel = 0.0f;
@@ -792,7 +792,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             cold.setf(kCAe, -10.0f);
           }
           const float3 d0 = make_float3(cold.f(kCDx), cold.f(kCDy), cold.f(kCDz));
-          emit_second(rng, background, d0, ph.dir);
+          emit_second<(kMode & kModeFast) != 0>(rng, background, d0, ph.dir);
           ph.pos = make_float3(cold.f(kCOx), cold.f(kCOy), cold.f(kCOz));
           which = 2;
           start_photon(TG, kAnnihilation);
@@ -1213,7 +1213,7 @@ __global__ void __launch_bounds__(kBlock) grad_replay_kernel(TransportParams P, 
     a.travel = 0.0f;
     a.state = 0;
     const bool esc_a = track_photon<false, kMode>(rng, P, T, T.palette, cmp, rn, a, cnt, &h);
-    emit_second(rng, background, dir0, b.dir);
+    emit_second<(kMode & kModeFast) != 0>(rng, background, dir0, b.dir);
     b.pos = origin;
     b.energy = kAnnihilation;
     b.travel = 0.0f;
