@@ -202,7 +202,8 @@ def test_neighbourhood_activity_derivatives_match_crn_finite_differences(c4):
     1.013, summed derivative within 1.4 %, median difference 1.6 %."""
     mat, act = c4["mat"], c4["act"]
     rng = np.random.default_rng(64)
-    centres = rng.choice(act.size, 64, replace=False, p=(act.ravel() / act.sum()).astype(np.float64))
+    w = act.ravel().astype(np.float64)
+    centres = rng.choice(act.size, 64, replace=False, p=w / w.sum())
     seed = C4_SEEDS[0]
     adj, fd = [], []
     for c in centres:
