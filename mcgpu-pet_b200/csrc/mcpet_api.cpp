@@ -543,6 +543,7 @@ int run_mode(const mcpet_scene* sc, const mcpet_run_opts& o) {
   if (o.lane_mode == MCPET_LANES_BALANCED) m |= kTransportFast;
   if (sc->cfg.prompt_gamma_energy > 0.0f) m |= kTransportPrompt;
   if (o.max_woodcock_steps > 0 || o.max_rejections > 0) m |= kTransportCaps;
+  if (sc->cfg.tally_psf_sinogram == 2) m |= kTransportSinogramOnly;
   return m;
 }
 
@@ -947,8 +948,10 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   }
   if (o.max_woodcock_steps > 0 || o.max_rejections > 0)
     return set_error(MCPET_ERR_ARG, "lowered loop caps are available for single-scene runs only");
+  bool sino_only = true;
+  for (const SceneSlot& z : L.slots) sino_only = sino_only && z.P.tally_psf_sinogram == 2;
   L.mode = (o.lane_mode == MCPET_LANES_BALANCED ? kTransportFast : 0) |
-           (L.P.prompt_energy > 0.0f ? kTransportPrompt : 0);
+           (L.P.prompt_energy > 0.0f ? kTransportPrompt : 0) | (sino_only ? kTransportSinogramOnly : 0);
   CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.share, L.mode, L.block, L.smem, &bps));
   if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", L.smem);
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;

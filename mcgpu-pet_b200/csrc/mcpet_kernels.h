@@ -20,6 +20,7 @@ constexpr int kAlgorithmEventsDose = 5;     /* event loop with the dose tallies 
 constexpr int kTransportFast = 1;
 constexpr int kTransportPrompt = 2;
 constexpr int kTransportCaps = 4;
+constexpr int kTransportSinogramOnly = 8;   /* no PSF tally (and no sinogram-dry PSF replays) */
 
 size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();
