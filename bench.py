@@ -285,8 +285,8 @@ def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, re
         return e0.elapsed_time(e1), time.perf_counter() - t0
 
     # each configuration runs once untimed first: a scene caches one lane
-    # plan, and the single runs and the batch size their automatic lanes
-    # differently, so a change of configuration rebuilds the plans on the host
+    # plan, and a change of options (the tuned histories per lane) rebuilds
+    # it on the host
     for s, t in zip(sc, tal):
         s.run_device(t, opts)
     seq_ms, seq_wall = timed(lambda: [s.run_device(t, opts) for s, t in zip(sc, tal)])

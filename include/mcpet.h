@@ -251,22 +251,25 @@ mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
                               mcpet_tallies* device_out);
 
 /* Batched run: the lanes of n_scenes scenes (phantoms of any size, each with
- * its own activity, seed, acquisition time and isotope mean life) in ONE
- * persistent launch of the transport kernel, so the GPU stays full through
+ * its own activity, seed, acquisition time and isotope mean life) in
+ * persistent launches of the transport kernel that keep the GPU full through
  * the tail of every scene.  Replaces n_scenes sequential runs of the
  * reference program (MCGPU-PET.cu:77-840, one phantom per process).  Each
  * scene keeps its own lane plan and RANECU streams: its tallies equal those
- * of mcpet_run on that scene alone with the same options.  The scenes must
- * use the same material files in the same slots (the Compton and Rayleigh
- * tables are shared by the launch) and sit on one device (scenes not yet on
- * a device are placed on scene 0's).  opts applies to every scene
- * (algorithm 0 or 2 only); with automatic histories per lane (<= 0) the
- * batch sizes its balanced lanes from all scenes' decays, which share the
- * GPU, so a scene's tallies equal mcpet_run of it alone with that explicit
- * value.  outs[k] receives scene k's tallies as in
- * mcpet_run; counters, when requested, are totals of the launch and go to
- * outs[0], and mcpet_last_run_guard(scenes[0]) reports the launch's guard
- * trips.  Blocking. */
+ * of mcpet_run on that scene alone with the same options (with automatic
+ * histories per lane, <= 0, every scene gets its own automatic lanes).  A
+ * scene of at least 2e7 decays whose lanes fill the GPU twice over runs as
+ * a launch of its own, with its own tables; the other scenes share one
+ * launch.  The launches follow one another on the stream, each allowed to
+ * start placing blocks (programmatic dependent launch) while the previous
+ * one drains its last lanes.  The scenes must use the same material files
+ * in the same slots (the shared launch reads one Compton and Rayleigh table
+ * for all) and sit on one device (scenes not yet on a device are placed on
+ * scene 0's).  opts applies to every scene (algorithm 0 or 2 only).
+ * outs[k] receives scene k's tallies as in mcpet_run; counters, when
+ * requested, are totals of all the launches and go to outs[0], and
+ * mcpet_last_run_guard(scenes[0]) reports the launches' guard trips.
+ * Blocking. */
 mcpet_status mcpet_run_batch(mcpet_scene* const* scenes, int n_scenes, const mcpet_run_opts* opts,
                              mcpet_tallies* outs);
 
@@ -369,11 +372,14 @@ mcpet_status mcpet_run_wait(mcpet_scene* scene);
  * decays (f = sample_decays / total decays, raised so that every candidate
  * keeps at least one decay per lane; sample_decays <= 0 means 2e8).
  * Candidates: 1/4, 1/2, 1, 2 and 4 times the automatic histories per lane of
- * the workload (for several scenes, the batch's: from all their decays) at
- * the full block, then smaller blocks at the best of those.  Runs go through mcpet_run_device (one scene) or
+ * the workload (for several scenes: sized from all their decays together)
+ * and, for several scenes, the automatic choice itself (every scene its own
+ * automatic lanes), at the full block, then smaller blocks at the best of
+ * those.  Runs go through mcpet_run_device (one scene) or
  * mcpet_run_batch_device (several) with opts and overwrite device_outs.  The
  * scenes' own settings are restored.  The result goes into
- * opts->histories_per_lane / block_threads of later runs; with reference
+ * opts->histories_per_lane / block_threads of later runs (a batch's
+ * histories_per_lane is 0 when the automatic choice won); with reference
  * lanes only the block size is tuned. */
 typedef struct {
   int block_threads;              /* chosen threads per block */
@@ -392,10 +398,11 @@ mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpe
  * Repeated runs of the same scenes (iterative reconstruction, Monte Carlo
  * averaging over seeds) need new histories every time, not new parameters.
  * mcpet_batch_graph_create builds the batch once, as mcpet_run_batch_device
- * does (the lane plans, the union tables, one launch of the event kernel over
- * every scene's lanes), keeps its own copies of the lane plans and tables on
- * the device, and captures into one CUDA graph: the zeroing of
- * device_outs[k], the transport launch, and a step of every scene's seed.
+ * does (the lane plans, the union tables, the launches of the event kernel
+ * over every scene's lanes), keeps its own copies of the lane plans and the
+ * union tables on the device, and captures into one CUDA graph: the zeroing
+ * of device_outs[k], the transport launches, and a step of every scene's
+ * seed.
  * Each mcpet_batch_graph_launch then regenerates all histories with one graph
  * launch and no host work: launch r (counted from 0, or from the last
  * mcpet_batch_graph_set_seeds) runs scene k with seed s_k + r*seed_step

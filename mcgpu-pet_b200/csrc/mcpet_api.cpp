@@ -793,26 +793,47 @@ mcpet_status check_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   return merge_shared_tables(scenes, n, U ? *U : local);
 }
 
-/* Everything one batched launch needs, built on the host: the scenes' slots
- * (parameters, tables, tallies, first lane), the union Compton/Rayleigh
- * tables, the launch-wide parameters and the launch shape. */
+/* One launch of a batched run: a range of slots, its launch-wide
+ * parameters and tables, and its shape.  A scene with enough decays and
+ * lanes to fill the GPU by itself is a launch of its own ("solo": its own
+ * tables, no lookup of the scene per lane); the other scenes share one. */
+struct BatchGroup {
+  int first = 0, count = 0;         /* slots [first, first + count) */
+  TransportParams P;                /* launch-wide parameters (the group's lanes) */
+  DeviceTables T;
+  int share = 0;                    /* kBatchShareScanner | kBatchSharePhantom */
+  bool solo = false;
+  int grid = 1;
+  size_t smem = 0;
+};
+
+/* Everything one batched run needs, built on the host: the scenes' slots
+ * (parameters, tables, tallies, first lane within their launch), the union
+ * Compton/Rayleigh tables, and the launches. */
 struct BatchLaunch {
-  std::vector<SceneSlot> slots;     /* launch order: longest lanes first */
+  std::vector<SceneSlot> slots;     /* launch order: solo scenes, then the shared launch's (longest lanes first) */
   std::vector<int> scene_of;        /* scene index of each slot */
   std::vector<int> slot_of;         /* slot of each scene */
-  unsigned long long* counter_words = nullptr;  /* scene 0's counters (launch totals) */
+  std::vector<BatchGroup> groups;
+  unsigned long long* counter_words = nullptr;  /* scene 0's counters (totals of the run) */
   SharedTables U;
-  TransportParams P;
-  DeviceTables T;
   uint64_t total = 0;
   bool counters = false, dose = false;
-  int share = 0;                    /* kBatchShareScanner | kBatchSharePhantom */
-  int mode = 0;                     /* kernel variant (fast arithmetic, prompt gamma) */
-  int grid = 1, block = 0;
-  size_t smem = 0;
-  /* device blob: slots | Compton table | Rayleigh float rows | Rayleigh byte rows */
-  size_t off_cmp = 0, off_ray = 0, off_ray8 = 0, bytes = 0;
+  int mode = 0;                     /* kernel variant (fast arithmetic, prompt gamma, sinogram only) */
+  int block = 0;
+  /* device blob: slots | Compton table | Rayleigh float rows | Rayleigh byte rows | lane cursors */
+  size_t off_cmp = 0, off_ray = 0, off_ray8 = 0, off_cursor = 0, bytes = 0;
 };
+
+/* A scene of at least this many decays runs as a launch of its own when its
+ * lanes fill the GPU twice over. */
+constexpr double kSoloDecays = 2.0e7;
+
+/* Decays of a scene's full acquisition (also while the autotuner runs it on
+ * a sample). */
+double scene_decays(const mcpet_scene* sc) {
+  return emitting_activity(sc) * ((double)sc->cfg.acquisition_time_ps * 1e-12) / sc->tune_scale;
+}
 
 /* True when scene b has scene a's scanner: detector, sinogram, energy
  * window and tally settings, and the acquisition time of the PSF records
@@ -850,9 +871,7 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   L.slots.assign((size_t)n, SceneSlot{});
   int max_shells = 1;
   L.total = 0;
-  /* automatic lanes of a batch: sized from all scenes' decays, which share
-   * the GPU (the scenes run alone with this value give the same tallies) */
-  int batch_hpl = o.histories_per_lane;
+  std::vector<char> solo((size_t)n, 0);
   for (int k = 0; k < n; ++k) {
     mcpet_scene* sc = scenes[k];
     sc->dev.run_h2d = 0;
@@ -865,10 +884,14 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
                        s0->dev.device);
     s = upload_tables(sc);
     if (s != MCPET_OK) return s;
-    if (batch_hpl <= 0) batch_hpl = auto_hpl_of(std::vector<const mcpet_scene*>(scenes, scenes + n));
+    /* each scene's lanes as in a run of it alone with the same options
+     * (automatic: from its own decays), so its tallies equal that run's */
+    const int hpl = o.histories_per_lane > 0 ? o.histories_per_lane : auto_hpl(sc);
     const int tpb = sc->cfg.threads_per_block > 0 ? sc->cfg.threads_per_block : 32;
-    s = build_lanes(sc, o.lane_mode, tpb, batch_hpl, st);
+    s = build_lanes(sc, o.lane_mode, tpb, hpl, st);
     if (s != MCPET_OK) return s;
+    const double resident = (double)std::max(sc->dev.sm_count, 1) * 2048.0;
+    solo[(size_t)k] = scene_decays(sc) >= kSoloDecays && (double)sc->dev.n_lanes >= 2.0 * resident;
     SceneSlot& z = L.slots[(size_t)k];
     memset(&z, 0, sizeof(z));
     z.O = outs[k];
@@ -881,13 +904,17 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
     z.T = device_tables(sc);
     max_shells = std::max(max_shells, z.P.max_shells);
   }
+  if (o.max_woodcock_steps > 0 || o.max_rejections > 0)
+    return set_error(MCPET_ERR_ARG, "lowered loop caps are available for single-scene runs only");
   CUDA_TRY(cudaSetDevice(s0->dev.device));
-  /* launch order: scenes with longer lanes first, so that no scene's longest
-   * lanes start near the end of the launch (each scene's plan is itself
-   * ordered longest first); results do not depend on the order */
+  /* launch order: the solo scenes, then the shared launch with longer lanes
+   * first, so that no scene's longest lanes start near the end of the
+   * launch (each scene's plan is itself ordered longest first); results do
+   * not depend on the order */
   L.scene_of.resize((size_t)n);
   for (int k = 0; k < n; ++k) L.scene_of[(size_t)k] = k;
   std::stable_sort(L.scene_of.begin(), L.scene_of.end(), [&](int a, int b) {
+    if (solo[(size_t)a] != solo[(size_t)b]) return solo[(size_t)a] > solo[(size_t)b];
     return scenes[a]->dev.max_lane_decays > scenes[b]->dev.max_lane_decays;
   });
   {
@@ -899,63 +926,81 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
       const int k = L.scene_of[(size_t)j];
       L.slots[(size_t)j] = by_scene[(size_t)k];
       L.slot_of[(size_t)k] = j;
-      L.slots[(size_t)j].first_lane = L.total;
-      L.total += scenes[k]->dev.n_lanes;
     }
+  }
+  /* the launches: one per solo scene, one for the rest; lanes numbered
+   * within a launch */
+  L.groups.clear();
+  for (int j = 0; j < n;) {
+    BatchGroup g;
+    g.first = j;
+    g.solo = solo[(size_t)L.scene_of[(size_t)j]] != 0;
+    g.count = g.solo ? 1 : n - j;
+    uint64_t lanes = 0;
+    for (int i = j; i < j + g.count; ++i) {
+      L.slots[(size_t)i].first_lane = lanes;
+      lanes += L.slots[(size_t)i].P.n_lanes;
+    }
+    L.total += lanes;
+    g.P = L.slots[(size_t)j].P;
+    g.P.n_lanes = lanes;
+    g.P.n_emitters = 0;
+    g.P.max_shells = max_shells;
+    /* the launch's shared layout holds the prompt-gamma fields when any of
+     * its scenes emits one (each lane reads its own scene's emitter) */
+    for (int i = j; i < j + g.count; ++i)
+      g.P.prompt_energy = std::max(g.P.prompt_energy, L.slots[(size_t)i].P.prompt_energy);
+    g.T = L.slots[(size_t)j].T;
+    g.T.emitters = nullptr;
+    L.groups.push_back(g);
+    j += g.count;
   }
 
   const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
   L.off_cmp = ((L.slots.size() * sizeof(SceneSlot) + 255) / 256) * 256;
   L.off_ray = L.off_cmp + ((sizeof(ComptonTable) + 255) / 256) * 256;
   L.off_ray8 = L.off_ray + 4 * nr * sizeof(float);
-  L.bytes = L.off_ray8 + 2 * nr;
+  L.off_cursor = ((L.off_ray8 + 2 * nr + 255) / 256) * 256;
+  L.bytes = L.off_cursor + L.groups.size() * sizeof(unsigned long long);
 
-  /* launch-wide view: lane count, the union tables (pointers set once the
-   * blob is on the device) */
-  L.P = L.slots[0].P;
-  L.P.n_lanes = L.total;
-  L.P.n_emitters = 0;
-  L.P.max_shells = max_shells;
-  /* the launch's shared layout holds the prompt-gamma fields when any scene
-   * emits one (each lane reads its own scene's emitter) */
-  for (const SceneSlot& z : L.slots) L.P.prompt_energy = std::max(L.P.prompt_energy, z.P.prompt_energy);
-  L.T = L.slots[0].T;
-  L.T.emitters = nullptr;
   L.counters = o.collect_counters && outs[0].counters;
   L.counter_words = L.counters ? outs[0].counters : nullptr;
   L.block = pick_block(o);
-  L.smem = transport_batch_dynamic_smem(L.P, L.block);
-  int bps = 0;
   L.dose = false;
   for (const SceneSlot& z : L.slots) L.dose = L.dose || z.O.mat_dose || z.O.vox_dose;
-  L.share = 0;
-  if (!L.counters && !L.dose) {
-    bool scanner = true, phantom = true;
-    for (int k = 1; k < n; ++k) {
-      scanner = scanner && same_scanner(L.slots[0].P, L.slots[(size_t)k].P);
-      phantom = phantom && same_phantom(s0, scenes[k]);
-    }
-    L.share = (scanner ? kBatchShareScanner : 0) | (phantom ? kBatchSharePhantom : 0);
+  bool sino_only = true, prompt = false;
+  for (const SceneSlot& z : L.slots) {
+    sino_only = sino_only && z.P.tally_psf_sinogram == 2;
+    prompt = prompt || z.P.prompt_energy > 0.0f;
   }
-  /* a shared phantom's palette is staged in shared memory, as in a single run */
-  if (L.share & kBatchSharePhantom) {
-    TransportParams one;
-    fill_params(s0, one);
-    if (one.palette_in_shared) {
-      L.P.palette_in_shared = one.palette_in_shared;
-      L.smem = transport_batch_dynamic_smem(L.P, L.block);
+  L.mode = (o.lane_mode == MCPET_LANES_BALANCED ? kTransportFast : 0) | (prompt ? kTransportPrompt : 0) |
+           (sino_only ? kTransportSinogramOnly : 0);
+  for (BatchGroup& g : L.groups) {
+    g.share = 0;
+    if (!L.counters && !L.dose) {
+      bool scanner = true, phantom = true;
+      for (int i = g.first + 1; i < g.first + g.count; ++i) {
+        scanner = scanner && same_scanner(L.slots[(size_t)g.first].P, L.slots[(size_t)i].P);
+        phantom = phantom && same_phantom(scenes[L.scene_of[(size_t)g.first]], scenes[L.scene_of[(size_t)i]]);
+      }
+      g.share = (scanner ? kBatchShareScanner : 0) | (phantom ? kBatchSharePhantom : 0);
     }
+    g.smem = transport_batch_dynamic_smem(g.P, L.block);
+    /* a shared phantom's palette is staged in shared memory, as in a single run */
+    if (g.share & kBatchSharePhantom) {
+      TransportParams one;
+      fill_params(scenes[L.scene_of[(size_t)g.first]], one);
+      if (one.palette_in_shared) {
+        g.P.palette_in_shared = one.palette_in_shared;
+        g.smem = transport_batch_dynamic_smem(g.P, L.block);
+      }
+    }
+    int bps = 0;
+    CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, g.share, L.mode, L.block, g.smem, &bps));
+    if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", g.smem);
+    if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
+    g.grid = g.P.n_lanes == 0 ? 1 : s0->dev.sm_count * bps;
   }
-  if (o.max_woodcock_steps > 0 || o.max_rejections > 0)
-    return set_error(MCPET_ERR_ARG, "lowered loop caps are available for single-scene runs only");
-  bool sino_only = true;
-  for (const SceneSlot& z : L.slots) sino_only = sino_only && z.P.tally_psf_sinogram == 2;
-  L.mode = (o.lane_mode == MCPET_LANES_BALANCED ? kTransportFast : 0) |
-           (L.P.prompt_energy > 0.0f ? kTransportPrompt : 0) | (sino_only ? kTransportSinogramOnly : 0);
-  CUDA_TRY(transport_batch_occupancy(L.counters, L.dose, L.share, L.mode, L.block, L.smem, &bps));
-  if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", L.smem);
-  if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
-  L.grid = L.total == 0 ? 1 : s0->dev.sm_count * bps;
   return MCPET_OK;
 }
 
@@ -970,46 +1015,54 @@ std::vector<unsigned char> batch_blob(const BatchLaunch& L) {
   return host;
 }
 
-/* Point the launch-wide tables at the blob on the device. */
+/* Point the launch-wide tables of the shared launch at the union tables in
+ * the blob on the device (a solo scene's launch reads its own tables). */
 void bind_blob(BatchLaunch& L, unsigned char* dbuf) {
   const size_t nr = (size_t)kMaxMaterials * kNpRayleigh;
-  L.T.compton = reinterpret_cast<const ComptonTable*>(dbuf + L.off_cmp);
-  const float* ray = reinterpret_cast<const float*>(dbuf + L.off_ray);
-  L.T.rayleigh.xco = ray;
-  L.T.rayleigh.pco = ray + nr;
-  L.T.rayleigh.aco = ray + 2 * nr;
-  L.T.rayleigh.bco = ray + 3 * nr;
-  L.T.rayleigh.itl = dbuf + L.off_ray8;
-  L.T.rayleigh.itu = dbuf + L.off_ray8 + nr;
+  for (BatchGroup& g : L.groups) {
+    if (g.solo) continue;
+    g.T.compton = reinterpret_cast<const ComptonTable*>(dbuf + L.off_cmp);
+    const float* ray = reinterpret_cast<const float*>(dbuf + L.off_ray);
+    g.T.rayleigh.xco = ray;
+    g.T.rayleigh.pco = ray + nr;
+    g.T.rayleigh.aco = ray + 2 * nr;
+    g.T.rayleigh.bco = ray + 3 * nr;
+    g.T.rayleigh.itl = dbuf + L.off_ray8;
+    g.T.rayleigh.itu = dbuf + L.off_ray8 + nr;
+  }
 }
 
-/* Stream work of one batched launch: zero the scenes' outputs and the
- * launch words (guard, lane cursor, counters), then the kernel. */
+/* Stream work of one batched run: zero the scenes' outputs and the run
+ * words (guard, counters, one lane cursor per launch in the blob), then the
+ * launches, each after the first allowed to start placing blocks while the
+ * previous one drains. */
 mcpet_status enqueue_batch_launch(mcpet_scene* const* scenes, int n, BatchLaunch& L, unsigned char* dbuf,
-                                  unsigned long long* guard, unsigned long long* cursor, cudaStream_t st,
-                                  cudaEvent_t ev0 = nullptr, cudaEvent_t ev1 = nullptr) {
+                                  unsigned long long* guard, cudaStream_t st, cudaEvent_t ev0 = nullptr,
+                                  cudaEvent_t ev1 = nullptr) {
   for (int k = 0; k < n; ++k) {
     mcpet_status s = zero_outputs(scenes[k], L.slots[(size_t)L.slot_of[(size_t)k]].O, st);
     if (s != MCPET_OK) return s;
   }
-  DeviceTallies O;
-  memset(&O, 0, sizeof(O));
-  O.guard = guard;
-  O.lane_cursor = cursor;
+  unsigned long long* cursors = reinterpret_cast<unsigned long long*>(dbuf + L.off_cursor);
   CUDA_TRY(cudaMemsetAsync(guard, 0, sizeof(unsigned long long), st));
-  CUDA_TRY(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
-  if (L.counters) {
-    O.counters = L.counter_words;
-    CUDA_TRY(cudaMemsetAsync(O.counters, 0, 10 * 8, st));
-  }
+  CUDA_TRY(cudaMemsetAsync(cursors, 0, L.groups.size() * sizeof(unsigned long long), st));
+  if (L.counters) CUDA_TRY(cudaMemsetAsync(L.counter_words, 0, 10 * 8, st));
   if (ev0) CUDA_TRY(cudaEventRecord(ev0, st));
-  CUDA_TRY(launch_transport_batch(L.P, L.T, O, reinterpret_cast<const SceneSlot*>(dbuf), n, L.counters, L.dose,
-                                  L.share, L.mode, L.grid, L.block, L.smem, st));
+  for (size_t i = 0; i < L.groups.size(); ++i) {
+    const BatchGroup& g = L.groups[i];
+    DeviceTallies O;
+    memset(&O, 0, sizeof(O));
+    O.guard = guard;
+    O.lane_cursor = cursors + i;
+    O.counters = L.counter_words;
+    CUDA_TRY(launch_transport_batch(g.P, g.T, O, reinterpret_cast<const SceneSlot*>(dbuf) + g.first, g.count,
+                                    L.counters, L.dose, g.share, L.mode, g.grid, L.block, g.smem, i > 0, st));
+  }
   if (ev1) CUDA_TRY(cudaEventRecord(ev1, st));
   return MCPET_OK;
 }
 
-/* Enqueue ONE launch of the event kernel over the lanes of all scenes.
+/* Enqueue the launches of the event kernel over the lanes of all scenes.
  * outs[k] are scene k's device tallies.  Each scene keeps its own lane plan
  * (cached on the scene like a single run's), seed and RANECU stream numbers,
  * so its tallies equal those of a run of that scene alone. */
@@ -1033,11 +1086,11 @@ mcpet_status enqueue_batch(mcpet_scene* const* scenes, int n, const mcpet_run_op
   s0->dev.last_h2d += (long long)L.bytes;
   bind_blob(L, dbuf);
   auto& d = s0->dev;
-  /* the launch's guard and work queue are scene 0's words */
+  /* the run's guard is scene 0's word */
   for (int k = 0; k < n; ++k) scenes[k]->dev.last_run_noalloc = false;
   for (int k = 1; k < n; ++k) CUDA_TRY(cudaMemsetAsync(scenes[k]->dev.small, 0, sizeof(unsigned long long), st));
-  s = enqueue_batch_launch(scenes, n, L, dbuf, d.small + 0, d.small + 1, st,
-                           ms_out ? (cudaEvent_t)d.ev0 : nullptr, ms_out ? (cudaEvent_t)d.ev1 : nullptr);
+  s = enqueue_batch_launch(scenes, n, L, dbuf, d.small + 0, st, ms_out ? (cudaEvent_t)d.ev0 : nullptr,
+                           ms_out ? (cudaEvent_t)d.ev1 : nullptr);
   if (s != MCPET_OK) {
     cudaFreeAsync(dbuf, st);
     return s;
@@ -1488,9 +1541,9 @@ struct mcpet_batch_graph {
   int device = -1;
   std::vector<mcpet_scene*> scenes;
   BatchLaunch L;
-  unsigned char* dbuf = nullptr;              /* slots + union tables */
+  unsigned char* dbuf = nullptr;              /* slots + union tables + lane cursors */
   mcpet::Emitter* plans = nullptr;            /* copies of the scenes' lane plans */
-  unsigned long long* words = nullptr;        /* guard, lane cursor, default coincidence words */
+  unsigned long long* words = nullptr;        /* guard, (unused), default coincidence words */
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   ~mcpet_batch_graph() {
@@ -1557,7 +1610,7 @@ mcpet_status mcpet_batch_graph_create(mcpet_scene* const* scenes, int n_scenes, 
   CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
   cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    s = enqueue_batch_launch(scenes, n_scenes, L, g->dbuf, g->words + 0, g->words + 1, cap);
+    s = enqueue_batch_launch(scenes, n_scenes, L, g->dbuf, g->words + 0, cap);
     if (s == MCPET_OK) {
       cudaError_t le = launch_advance_seeds(reinterpret_cast<SceneSlot*>(g->dbuf), n_scenes, seed_step, cap);
       if (le != cudaSuccess) s = set_error(MCPET_ERR_CUDA, "CUDA error: %s", cudaGetErrorString(le));
@@ -1603,22 +1656,25 @@ mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpe
                                                           : ensure_device(scenes[k]);
     if (s != MCPET_OK) return s;
   }
-  /* decays of the workload and its automatic histories per lane (the
-   * batch's, from all scenes' decays): the centre of the candidates */
+  /* decays of the workload; the candidates: 1/4 ... 4 times the histories
+   * per lane sized from all scenes' decays together and, for a batch, the
+   * automatic choice (0: every scene its own automatic lanes).  With
+   * reference lanes the plan is fixed and only the block size is tuned. */
   double D = 0;
   for (int k = 0; k < n_scenes; ++k)
     D += emitting_activity(scenes[k]) * ((double)scenes[k]->cfg.acquisition_time_ps * 1e-12);
   const int base = auto_hpl_of(std::vector<const mcpet_scene*>(scenes, scenes + n_scenes));
-  std::vector<int> hpls;
+  const int auto_choice = (balanced && n_scenes == 1) ? base : 0;
+  std::vector<int> hpls(1, auto_choice);
+  int smallest = 0;
   if (balanced) {
     const int c[5] = {std::max(1, base / 4), std::max(1, base / 2), base, 2 * base, 4 * base};
+    smallest = c[0];
     for (int v : c)
       if (std::find(hpls.begin(), hpls.end(), v) == hpls.end()) hpls.push_back(v);
-  } else {
-    hpls.push_back(0);   /* reference lanes: the plan is fixed, only the block size is tuned */
   }
   double f = (sample_decays > 0 ? sample_decays : 2.0e8) / std::max(D, 1.0);
-  if (balanced) f = std::max(f, 1.0 / (double)hpls.front());
+  if (balanced) f = std::max(f, 1.0 / (double)smallest);
   if (f > 1.0) f = 1.0;
   out->sample_fraction = f;
 
@@ -1626,13 +1682,14 @@ mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpe
   for (int k = 0; k < n_scenes; ++k) {
     acq[(size_t)k] = scenes[k]->cfg.acquisition_time_ps;
     scenes[k]->cfg.acquisition_time_ps = (unsigned long long)llround((double)acq[(size_t)k] * f);
+    scenes[k]->tune_scale = f;   /* a batch groups the scenes by their full decays */
     scenes[k]->dev.activity_dirty = true;
   }
   std::vector<DeviceTallies> outs((size_t)n_scenes);
   cudaStream_t st = (cudaStream_t)o.stream;
   auto time_one = [&](int hpl, int block, double* ms) -> mcpet_status {
     mcpet_run_opts c = o;
-    c.histories_per_lane = balanced ? std::max(1, (int)llround(hpl * f)) : 0;
+    c.histories_per_lane = (balanced && hpl > 0) ? std::max(1, (int)llround(hpl * f)) : 0;
     c.block_threads = block;
     for (int k = 0; k < n_scenes; ++k) outs[(size_t)k] = tallies_from(&device_outs[k]);
     if (n_scenes == 1) return enqueue_run(scenes[0], &c, outs[0], st, ms);
@@ -1642,11 +1699,11 @@ mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpe
   double best = 1e300, ms = 0;
   int best_hpl = hpls[0], best_block = transport_block_threads();
   /* first the histories per lane at the full block, then the block size */
-  s = time_one(base, best_block, &ms);   /* warm-up: clocks, tables, first plan */
+  s = time_one(auto_choice, best_block, &ms);   /* warm-up: clocks, tables, first plan */
   for (size_t i = 0; s == MCPET_OK && i < hpls.size(); ++i) {
     s = time_one(hpls[i], transport_block_threads(), &ms);
     ++out->candidates;
-    if (s == MCPET_OK && hpls[i] == (balanced ? base : 0)) out->auto_ms = ms;
+    if (s == MCPET_OK && hpls[i] == auto_choice) out->auto_ms = ms;
     if (s == MCPET_OK && ms < best) {
       best = ms;
       best_hpl = hpls[i];
@@ -1664,10 +1721,11 @@ mcpet_status mcpet_autotune(mcpet_scene* const* scenes, int n_scenes, const mcpe
   }
   for (int k = 0; k < n_scenes; ++k) {
     scenes[k]->cfg.acquisition_time_ps = acq[(size_t)k];
+    scenes[k]->tune_scale = 1.0;
     scenes[k]->dev.activity_dirty = true;
   }
   if (s != MCPET_OK) return s;
-  out->histories_per_lane = balanced ? best_hpl : 0;
+  out->histories_per_lane = balanced ? best_hpl : 0;   /* 0 for a batch: the automatic choice won */
   out->block_threads = best_block;
   out->best_ms = best;
   return MCPET_OK;

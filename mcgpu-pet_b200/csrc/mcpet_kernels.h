@@ -41,7 +41,7 @@ cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int m
                                       int* blocks_per_sm);
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                                    const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int mode,
-                                   int grid, int block, size_t smem, cudaStream_t stream);
+                                   int grid, int block, size_t smem, bool after_previous, cudaStream_t stream);
 
 /* batched regeneration: advance every slot's RANECU seed by `step` within
  * [1, m1 - 1] (the next replay of a captured batch) */

@@ -40,10 +40,24 @@ cudaError_t transport_batch_occupancy(bool counters, bool dose, int share, int m
 
 cudaError_t launch_transport_batch(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                                    const SceneSlot* slots, int n_slots, bool counters, bool dose, int share, int mode,
-                                   int grid, int block, size_t smem, cudaStream_t stream) {
+                                   int grid, int block, size_t smem, bool after_previous, cudaStream_t stream) {
   EventKernel k = batch_event_kernel(counters, dose, share, mode);
   if (!k) return cudaErrorNotSupported;
-  k<<<grid, block, smem, stream>>>(P, T, O, slots, n_slots);
+  /* after_previous: the launch may start placing blocks while the previous
+   * launch on the stream drains its last lanes (programmatic dependent
+   * launch; the kernel signals it once a block runs out of lanes) */
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = after_previous ? 1 : 0;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k, P, T, O, slots, n_slots);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

@@ -111,6 +111,9 @@ struct mcpet_scene {
     long long run_h2d = 0;        /* host->device bytes of the run in progress */
     long long last_h2d = 0;       /* ... and of the last completed run */
   } dev;
+  /* the autotuner runs scenes on a sample of their decays: the fraction, so
+   * that a batch still groups them by their full decays */
+  double tune_scale = 1.0;
 
   ~mcpet_scene();
 };

@@ -998,6 +998,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
     }
   }
 
+  /* a batched run's next launch may start placing its blocks as this
+   * grid's blocks run out of lanes (programmatic dependent launch) */
+  if (kBatch) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (kBatch) {
     flush_lane();
   } else {
@@ -1023,6 +1026,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
       if (spec_sh[i]) atomicAdd(&O.spectrum[i], spec_sh[i]);
   if (kDose && !kBatch && O.mat_dose && threadIdx.x < 2 * kMaxMaterials && mdose_sh[threadIdx.x])
     atomicAdd(&O.mat_dose[threadIdx.x], mdose_sh[threadIdx.x]);
+  /* ... and does not complete before the previous launch has (all of whose
+   * blocks are resident or done once this grid runs), so the stream's later
+   * work sees every launch of the run finished; a no-op without a
+   * programmatic dependency */
+  if (kBatch) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 /* ---------------------------------------------------------- launch helpers */

@@ -1,6 +1,7 @@
 """Batched runs (mcpet_run_batch / mcpet_run_batch_device): several phantoms of
 uneven size, each with its own activity, seed, acquisition time and isotope
-mean life, in ONE launch of the transport kernel.  Every scene keeps its own
+mean life, in one launch of the transport kernel (large scenes in chained
+launches of their own).  Every scene keeps its own
 lane plan and RANECU streams, so its tallies must equal those of the same
 scene run alone: compared bit for bit, in both lane layouts."""
 import numpy as np
@@ -50,6 +51,41 @@ def test_batch_equals_runs_one_by_one(tmp_path, lanes):
     again = mcpet.Scene.run_batch(sc, opts)
     for k, (a, b) in enumerate(zip(batch, again)):
         _same(a, b, f"repeat scene {k}")
+    for s in sc:
+        s.close()
+
+
+def _with_large_scenes(tmp):
+    """The small scenes plus two heads of 2.5e7 and 3e7 decays: enough decays
+    and lanes for launches of their own."""
+    out = _batch_scenes(tmp)
+    for k, (bq, seed) in enumerate(((2.5e7, 99), (3.0e7, 98))):
+        mat, rho, act, vs, _ = inputs.head_phantom(shape=(40, 64, 64), voxel_cm=0.4, seed=20 + k, total_bq=bq)
+        out.insert(1 + k, scenes.scene_from_arrays(str(tmp), mat, rho, act, vs, tissues=HEAD_TISSUES, seed=seed,
+                                                   **inputs.scanner_batch()))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lanes", [mcpet.LANES_REFERENCE, mcpet.LANES_BALANCED])
+def test_batch_with_chained_launches_equals_runs_one_by_one(tmp_path, lanes):
+    """The two large scenes run as launches of their own, chained on the
+    stream ahead of the launch the small scenes share; with automatic lanes
+    every scene gets its own, so each equals its run alone; counters are the
+    totals of all launches."""
+    import dataclasses
+    sc = _with_large_scenes(tmp_path)
+    opts = mcpet.RunOptions(lane_mode=lanes)
+    alone = [s.run(opts) for s in sc]
+    batch = mcpet.Scene.run_batch(sc, opts)
+    for k, (a, b) in enumerate(zip(alone, batch)):
+        _same(a, b, f"scene {k}")
+    copts = dataclasses.replace(opts, collect_counters=True)
+    counts = [s.run(copts).counters for s in sc]
+    first = mcpet.Scene.run_batch(sc, copts)[0]
+    for key in ("photons", "compton", "rayleigh", "photoelectric", "tally_increments", "lanes", "guard_trips"):
+        assert first.counters[key] == sum(c[key] for c in counts), key
+    assert first.counters["guard_trips"] == 0
     for s in sc:
         s.close()
 
