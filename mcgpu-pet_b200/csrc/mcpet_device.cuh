@@ -343,64 +343,67 @@ __device__ __forceinline__ float compton_s0(float E, int mat, const ComptonTable
   return s0;
 }
 
+/* One trial of GCOa's first stage (MCGPU-PET_kernel.cu:1390-1451): tau = E'/E
+ * from the Klein-Nishina-like envelope, then the rejection on the incoherent
+ * scattering function, normalised by s0 (compton_s0 of E and the material).
+ * Returns true on acceptance, with tau, cdt1 = 1 - cos(theta), the sum s and
+ * the shell terms rn[] that the second stage reads.  A trial draws the same
+ * random numbers whether the trials of one sampling run back to back or
+ * with other work of the thread between them. */
 template <typename Scratch>
-__device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, const ComptonTable& C,
-                                               Scratch rn, double& costh, const float* s0_annihilation = nullptr,
-                                               int max_rejections = kMaxRejections) {
-  const float E = energy;
+__device__ __forceinline__ bool compton_trial(Rng& r, float E, int mat, const ComptonTable& C, Scratch rn,
+                                              float s0, float& tau, float& s, double& cdt1) {
   const int nsh = C.noscco[mat];
   float ek = E * 1.956951306108245e-6f;
   float ek2 = ek * 2.f + 1.f;
   float ek3 = ek * ek;
   float taumin = 1.f / ek2;
   float a1 = logf(ek2);
-  const float s0 = (s0_annihilation && E == kAnnihilation) ? s0_annihilation[mat] : compton_s0(E, mat, C);
-
-  /* sample tau = E'/E with the Klein-Nishina-like envelope, reject on S */
-  float tau, s;
-  double cdt1;
-  int it = 0;
-  for (;;) {
-    if (++it > max_rejections) return false;
-    if (ranecu(r) * (a1 + 2. * ek * (ek + 1.f) * taumin * taumin) < a1) {
-      tau = powf(taumin, ranecu(r));
-    } else {
-      tau = sqrtf(1.f + ranecu(r) * (taumin * taumin - 1.f));
-    }
-    cdt1 = (double)(1.f - tau) / (((double)tau) * ((double)E) * 1.956951306108245e-6);
-    if (cdt1 > 2.0) cdt1 = 1.99999999;
-    s = 0.0f;
-    for (int i = 0; i < nsh; ++i) {
-      float u = C.uico[mat + i * kMaxMaterials];
-      if (u < E) {
-        float aux = E * (E - u) * ((float)cdt1);
-        float pz;
-        if ((aux > 1.0e-12f) || (u > 1.0e-12f)) {
-          pz = C.fj0[mat + i * kMaxMaterials] * (aux - u * 510998.918f) * rsqrtf(aux + aux + u * u) *
-               1.956951306108245e-6f;
-        } else {
-          pz = 0.002f;
-        }
-        float t = pz * 1.4142135623731f;
-        if (pz > 0.0f) t = 0.5f - (t + 0.70710678118654502f) * (t + 0.70710678118654502f);
-        else t = 0.5f - (0.70710678118654502f - t) * (0.70710678118654502f - t);
-        t = 0.5f * expf(t);
-        if (pz > 0.0f) t = 1.0f - t;
-        s += C.fco[mat + i * kMaxMaterials] * t;
-        rn[i] = t;
-      } else {
-        rn[i] = 0.0f;   /* shell above the photon energy: the reference leaves it uninitialised */
-      }
-    }
-    if (!((ranecu(r) * s0) >
-          (s * (1.0f + tau * ((ek3 - ek2 - 1.0f) + tau * (ek2 + tau * ek3)))) / (ek3 * tau * (tau * tau + 1.0f))))
-      break;
+  if (ranecu(r) * (a1 + 2. * ek * (ek + 1.f) * taumin * taumin) < a1) {
+    tau = powf(taumin, ranecu(r));
+  } else {
+    tau = sqrtf(1.f + ranecu(r) * (taumin * taumin - 1.f));
   }
-  costh = 1.0 - cdt1;
+  cdt1 = (double)(1.f - tau) / (((double)tau) * ((double)E) * 1.956951306108245e-6);
+  if (cdt1 > 2.0) cdt1 = 1.99999999;
+  s = 0.0f;
+  for (int i = 0; i < nsh; ++i) {
+    float u = C.uico[mat + i * kMaxMaterials];
+    if (u < E) {
+      float aux = E * (E - u) * ((float)cdt1);
+      float pz;
+      if ((aux > 1.0e-12f) || (u > 1.0e-12f)) {
+        pz = C.fj0[mat + i * kMaxMaterials] * (aux - u * 510998.918f) * rsqrtf(aux + aux + u * u) *
+             1.956951306108245e-6f;
+      } else {
+        pz = 0.002f;
+      }
+      float t = pz * 1.4142135623731f;
+      if (pz > 0.0f) t = 0.5f - (t + 0.70710678118654502f) * (t + 0.70710678118654502f);
+      else t = 0.5f - (0.70710678118654502f - t) * (0.70710678118654502f - t);
+      t = 0.5f * expf(t);
+      if (pz > 0.0f) t = 1.0f - t;
+      s += C.fco[mat + i * kMaxMaterials] * t;
+      rn[i] = t;
+    } else {
+      rn[i] = 0.0f;   /* shell above the photon energy: the reference leaves it uninitialised */
+    }
+  }
+  return !((ranecu(r) * s0) >
+           (s * (1.0f + tau * ((ek3 - ek2 - 1.0f) + tau * (ek2 + tau * ek3)))) / (ek3 * tau * (tau * tau + 1.0f)));
+}
 
-  /* target shell and projected momentum pz, with the F(EP) rejection */
+/* GCOa's second stage after an accepted trial (MCGPU-PET_kernel.cu:1453-1562):
+ * the target shell and projected momentum pz with the F(EP) rejection, then
+ * the energy of the scattered photon.  costh = 1 - cdt1 of the trial.
+ * Returns false when the rejection guard fired. */
+template <typename Scratch>
+__device__ __forceinline__ bool compton_doppler(Rng& r, float& energy, int mat, const ComptonTable& C, Scratch rn,
+                                                float tau, float s, double costh,
+                                                int max_rejections = kMaxRejections) {
+  const int nsh = C.noscco[mat];
   float pzomc, af;
-  it = 0;
+  int it = 0;
   for (;;) {
     if (++it > max_rejections) return false;
     float t = s * ranecu(r);
@@ -447,6 +450,24 @@ __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, c
     energy *= t;
   }
   return true;
+}
+
+/* The whole sampling: trials until one is accepted, then the second stage. */
+template <typename Scratch>
+__device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, const ComptonTable& C,
+                                               Scratch rn, double& costh, const float* s0_annihilation = nullptr,
+                                               int max_rejections = kMaxRejections) {
+  const float E = energy;
+  const float s0 = (s0_annihilation && E == kAnnihilation) ? s0_annihilation[mat] : compton_s0(E, mat, C);
+  float tau, s;
+  double cdt1;
+  int it = 0;
+  for (;;) {
+    if (++it > max_rejections) return false;
+    if (compton_trial(r, E, mat, C, rn, s0, tau, s, cdt1)) break;
+  }
+  costh = 1.0 - cdt1;
+  return compton_doppler(r, energy, mat, C, rn, tau, s, costh, max_rejections);
 }
 
 /* ------------------------------------------------------------------------

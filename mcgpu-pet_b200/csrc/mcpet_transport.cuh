@@ -540,6 +540,7 @@ enum : int {
   kCAe, kCAt, kCAs,                              /* photon 1 energy (-10 absorbed), travel, state */
   kCInvLo, kCInvHi, kCTLo, kCTHi, kCVox,         /* lane: 1/rate (double), remaining ps (u64), voxel */
   kCRx, kCRy,                                    /* RANECU state right before the pair's emission */
+  kCTrial, kCS0,                                 /* pending Compton sampling: trials so far, its s0 */
   kCHist, kCDet,                                 /* batch only: lane photons started, coincidences tallied */
   kCPmax,                                        /* batch only: Rayleigh pmax of the pending interaction */
   kCBx, kCBy, kCBz, kCBu, kCBv, kCBw,            /* prompt gamma only: photon 2 at exit: position, direction, */
@@ -672,6 +673,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
     cold.u(kCHist) = 0;
     cold.u(kCDet) = 0;
   }
+  cold.u(kCTrial) = 0;
   auto flush_lane = [&]() {
     if (!kBatch) return;
     const unsigned long long h = cold.u(kCHist), c = cold.u(kCDet);
@@ -728,20 +730,57 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
       /* ---- real scattering: Compton (MCGPU-PET_kernel.cu:351-373) or
        * Rayleigh (:375-387), then the common direction update.  Rayleigh
        * lanes (GRAa) join a round with Compton lanes only when at least
-       * quorum_rayleigh of them wait, so that most rounds run one sampler */
+       * quorum_rayleigh of them wait, so that most rounds run one sampler.
+       * The Compton lanes repeat trials of GCOa's first stage until at most
+       * an eighth of them are still rejected; those keep their phase and go
+       * on in a later round, with the lanes that arrive meanwhile, instead of
+       * holding the warp in the rejection loop (each lane draws its random
+       * numbers in the same order either way) */
       const unsigned m_ray = __ballot_sync(0xffffffffu, phase == kPhCompton && !is_compton);
+      const unsigned m_c = m_cmp & ~m_ray;
       const bool ray_now = (m_cmp == m_ray) || (__popc(m_ray) >= P.quorum_rayleigh);
       if (phase == kPhCompton && (is_compton || ray_now)) {
         double costh = 0.0;
-        bool ok;
+        bool ok = false, pending = false;
         float e = ph.energy;
         if (is_compton) {
-          ok = sample_compton(rng, e, mat0, cmp, rn, costh, s0_ann, rejections_cap<kMode>(P));
+          uint32_t trials = cold.u(kCTrial);
+          float s0;
+          if (e == kAnnihilation) {
+            s0 = s0_ann[mat0];
+          } else if (trials == 0) {
+            s0 = compton_s0(e, mat0, cmp);
+            cold.setf(kCS0, s0);
+          } else {
+            s0 = cold.f(kCS0);
+          }
+          float tau = 0.f, s = 0.f;
+          double cdt1 = 0.0;
+          bool accepted = false, tripped = false;
+          for (;;) {
+            if (!accepted && !tripped) {
+              if (++trials > (uint32_t)rejections_cap<kMode>(P)) tripped = true;
+              else accepted = compton_trial(rng, e, mat0, cmp, rn, s0, tau, s, cdt1);
+            }
+            if (8 * __popc(__ballot_sync(m_c, !accepted && !tripped)) <= __popc(m_c)) break;
+          }
+          if (accepted) {
+            cold.u(kCTrial) = 0;
+            costh = 1.0 - cdt1;
+            ok = compton_doppler(rng, e, mat0, cmp, rn, tau, s, costh, rejections_cap<kMode>(P));
+          } else if (tripped) {
+            cold.u(kCTrial) = 0;
+          } else {
+            cold.u(kCTrial) = trials;
+            pending = true;
+          }
         } else {
           ok = sample_rayleigh(rng, e, mat0, kBatch ? cold.f(kCPmax) : rec_hi.z, T.rayleigh, costh,
                                rejections_cap<kMode>(P));
         }
-        if (!ok) {
+        if (pending) {
+          /* next trial in a later scattering round */
+        } else if (!ok) {
           Counting<true>::add(cnt.guard, 1);
           escaped = false;
           phase = kPhEnd;
