@@ -143,7 +143,7 @@ void fill_params(const mcpet_scene* sc, TransportParams& P) {
   P.e_annihilation = 510998.95f;
   for (int k = 0; k < 6; ++k) P.dose_roi[k] = c.tally_voxel_dose ? c.dose_roi[k] : (k % 2 ? -1 : 0);
   P.quorum_scatter = env_int("MCPET_QUORUM_SCATTER", 16, 1, 32);
-  P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 32, 1, 32);
+  P.quorum_pair = env_int("MCPET_QUORUM_PAIR", 16, 1, 32);
   P.step_keep = env_int("MCPET_STEP_KEEP", 2, 1, 8);
   P.quorum_rayleigh = env_int("MCPET_QUORUM_RAYLEIGH", 2, 1, 32);
   P.max_steps = kMaxStepsDefault;
