@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
         double costh = 0.0;
         bool ok = false, pending = false;
         float e = ph.energy;
-        if (is_compton) {
+        if (__builtin_expect(is_compton, 1)) {
           uint32_t trials = cold.u(kCTrial);
           float s0;
           if (e == kAnnihilation) {
@@ -780,7 +780,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
         }
         if (pending) {
           /* next trial in a later scattering round */
-        } else if (!ok) {
+        } else if (__builtin_expect(!ok, 0)) {
           Counting<true>::add(cnt.guard, 1);
           escaped = false;
           phase = kPhEnd;
@@ -894,7 +894,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
       /* ---- next decay of the lane, or the next lane (MCGPU-PET_kernel.cu:259-298) */
       if (phase == kPhDecay) {
         for (;;) {
-          if (!lane_live) {
+          if (__builtin_expect(!lane_live, 0)) {   /* rare branches hinted: cold code out of the hot paths */
             const uint64_t lane = claim_lane(O.lane_cursor);
             if (lane >= n_lanes) {
               phase = kPhDone;
@@ -930,7 +930,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           double inv_act = cold.inv_rate();
           unsigned long long t_left = cold.t_left();
           const unsigned long long dt_ps = decay_interval<(kMode & kModeFast) != 0>(rng, inv_act, PN.inv_mean_life);
-          if (!(dt_ps < t_left)) {
+          if (__builtin_expect(!(dt_ps < t_left), 0)) {
             lane_live = false;
             continue;
           }
@@ -980,7 +980,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             if (vox < 0) {
               escaped = true;
               phase = kPhEnd;
-            } else if ((unsigned long long)vox >= (unsigned long long)PG.n_voxels || ++steps > steps_cap<kMode>(P)) {
+            } else if (__builtin_expect((unsigned long long)vox >= (unsigned long long)PG.n_voxels ||
+                                            ++steps > steps_cap<kMode>(P), 0)) {
               Counting<true>::add(cnt.guard, 1);
               escaped = false;
               phase = kPhEnd;
@@ -1003,13 +1004,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
               if (!(randno < prob)) {
                 /* real interaction: the record of (energy bin, material) holds
                  * the same values the reference cached at the last change */
-                const float4 lo = __ldg(reinterpret_cast<const float4*>(rec));
-                rec_hi = __ldg(reinterpret_cast<const float4*>(rec) + 1);
-                prob += mfp_density * (lo.z + E * lo.w);
-                if (randno < prob) {
+                const float2 cc = __ldg(rec + 1);   /* Compton coefficients; the rest only if needed */
+                prob += mfp_density * (cc.x + E * cc.y);
+                if (__builtin_expect(randno < prob, 1)) {
                   phase = kPhCompton;
                   is_compton = true;
                 } else {
+                  rec_hi = __ldg(reinterpret_cast<const float4*>(rec) + 1);
                   prob += mfp_density * (rec_hi.x + E * rec_hi.y);
                   if (randno < prob) {
                     phase = kPhCompton;
