@@ -175,6 +175,27 @@ void apply_caps(const mcpet_run_opts& o, TransportParams& P) {
   P.max_rejections = o.max_rejections > 0 ? o.max_rejections : kMaxRejectionsDefault;
 }
 
+/* GCOa's incoherent scattering function at theta = pi for energy E (eV) and
+ * material mat, in double precision: the normaliser of its rejection step
+ * (MCGPU-PET_kernel.cu:1366-1391; PENELOPE's analytical one-electron
+ * Compton profiles).  Non-decreasing in E: each shell's projected momentum
+ * at theta = pi grows with E, and so does its profile integral. */
+double compton_s0_host(double E, int mat, const ComptonTable& C) {
+  const double mc2 = 510998.918, inv_mc2 = 1.956951306108245e-6, r2 = 1.4142135623731, ir2 = 0.70710678118654502;
+  double s0 = 0.0;
+  for (int i = 0; i < C.noscco[mat]; ++i) {
+    const double u = C.uico[mat + i * kMaxMaterials];
+    if (u >= E) continue;
+    const double aux = E * (E - u) * 2.0;
+    const double pz = C.fj0[mat + i * kMaxMaterials] * (aux - u * mc2) / std::sqrt(aux + aux + u * u) * inv_mc2;
+    const double a = pz > 0.0 ? ir2 + pz * r2 : ir2 - pz * r2;
+    double t = 0.5 * std::exp(0.5 - a * a);
+    if (pz > 0.0) t = 1.0 - t;
+    s0 += C.fco[mat + i * kMaxMaterials] * t;
+  }
+  return s0;
+}
+
 mcpet_status upload_tables(mcpet_scene* sc) {
   auto& d = sc->dev;
   if (d.tables_ready) return MCPET_OK;
@@ -205,7 +226,15 @@ mcpet_status upload_tables(mcpet_scene* sc) {
     r.az = sc->mfp_a[3 * i + 2];
     r.bz = sc->mfp_b[3 * i + 2];
     r.pmax_next = (i + kMaxMaterials < nrec) ? sc->pmax[i + kMaxMaterials] : 0.0f;
-    r.pad = 0.f;
+    r.s0_bound = 0.f;
+    const int mat = (int)(i % kMaxMaterials);
+    if (sc->compton.noscco[mat] > 0) {
+      /* bin k holds the energies with floor((E - e0) * ide) = k: bound them by
+       * S at the upper edge of bin k + 1 (a margin for the float index) */
+      const double e_hi = (double)sc->e0 + (double)(i / kMaxMaterials + 2) / (double)sc->ide;
+      const float b = (float)(compton_s0_host(e_hi, mat, sc->compton) * (1.0 + 1e-5));
+      r.s0_bound = std::nextafter(b, 1e30f);
+    }
   }
   CUDA_TRY(dmalloc(&d.mfp, nrec * sizeof(MfpRecord)));
   CUDA_TRY(cudaMemcpy(d.mfp, rec.data(), nrec * sizeof(MfpRecord), cudaMemcpyHostToDevice));

@@ -452,13 +452,15 @@ __device__ __forceinline__ bool compton_doppler(Rng& r, float& energy, int mat, 
   return true;
 }
 
-/* The whole sampling: trials until one is accepted, then the second stage. */
+/* The whole sampling: trials until one is accepted, then the second stage.
+ * s0 < 0: the normaliser evaluated at the photon's energy (the reference's
+ * arithmetic); else the bound given (MfpRecord::s0_bound). */
 template <typename Scratch>
 __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, const ComptonTable& C,
-                                               Scratch rn, double& costh, const float* s0_annihilation = nullptr,
+                                               Scratch rn, double& costh, float s0_given = -1.0f,
                                                int max_rejections = kMaxRejections) {
   const float E = energy;
-  const float s0 = (s0_annihilation && E == kAnnihilation) ? s0_annihilation[mat] : compton_s0(E, mat, C);
+  const float s0 = s0_given < 0.0f ? compton_s0(E, mat, C) : s0_given;
   float tau, s;
   double cdt1;
   int it = 0;

@@ -21,7 +21,13 @@ constexpr int kSpectrumSharedMax = 4096; /* spectrum bins privatised in shared m
  * two 16-byte loads. */
 struct alignas(16) MfpRecord {
   float ax, bx, ay, by;
-  float az, bz, pmax_next, pad;
+  float az, bz, pmax_next;
+  /* An upper bound, over the energies of this bin, of GCOa's rejection
+   * normaliser S(E, theta = pi) of the material (its value two bin edges
+   * up, times 1 + 1e-5; it grows with E).  Balanced lanes divide by it
+   * instead of evaluating S(E, pi) per sampling: a larger constant in a
+   * rejection sampler leaves the accepted distribution unchanged. */
+  float s0_bound;
 };
 
 /* Distinct (material, density) pair of the phantom; voxels store an index. */

@@ -194,7 +194,8 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       /* Compton */
       double costh;
       const float e_before = energy;
-      if (!sample_compton(rng, energy, mat0, C, rn, costh, nullptr, rejections_cap<kMode>(P))) {
+      if (!sample_compton(rng, energy, mat0, C, rn, costh, (kMode & kModeFast) ? rec_hi.w : -1.0f,
+                          rejections_cap<kMode>(P))) {
         Counting<true>::add(cnt.guard, 1);
         ph.energy = energy;
         return false;
@@ -746,7 +747,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
         if (__builtin_expect(is_compton, 1)) {
           uint32_t trials = cold.u(kCTrial);
           float s0;
-          if (e == kAnnihilation) {
+          if (kMode & kModeFast) {
+            /* balanced lanes: the bin's bound of the normaliser */
+            s0 = __ldg(&TG.mfp[(size_t)index * kMaxMaterials + mat0].s0_bound);
+          } else if (e == kAnnihilation) {
             s0 = s0_ann[mat0];
           } else if (trials == 0) {
             s0 = compton_s0(e, mat0, cmp);
