@@ -502,7 +502,9 @@ mcpet_status mcpet_probe_rayleigh(const mcpet_scene* scene, int n, const float* 
                                   double* costh_out, int32_t* seeds_out);
 
 /* Photon-pair source (source :666-773) for every voxel of an nx*ny*nz grid:
- * out[12*v..] = position1, direction1, position2, direction2. */
+ * out[12*v..] = position1, direction1, position2, direction2.
+ * background_mode: 0 or 1 (isotropic second photon), plus 2 for the
+ * balanced lanes' photon-2 emission (same distribution, other arithmetic). */
 mcpet_status mcpet_probe_source(int nx, int ny, int nz, const float inv_voxel_size[3],
                                 int background_mode, const int32_t* seeds_in, float* out,
                                 int32_t* seeds_out);

@@ -2349,7 +2349,8 @@ mcpet_status mcpet_probe_rayleigh(const mcpet_scene* sc, int n, const float* ene
 
 mcpet_status mcpet_probe_source(int nx, int ny, int nz, const float inv_voxel_size[3], int background_mode,
                                 const int32_t* seeds_in, float* out, int32_t* seeds_out) {
-  if (nx <= 0 || ny <= 0 || nz <= 0 || !inv_voxel_size || !seeds_in || !out || !seeds_out)
+  if (nx <= 0 || ny <= 0 || nz <= 0 || !inv_voxel_size || !seeds_in || !out || !seeds_out ||
+      background_mode < 0 || background_mode > 3)
     return set_error(MCPET_ERR_ARG, "invalid probe arguments");
   mcpet_status s = probe_device();
   if (s != MCPET_OK) return s;

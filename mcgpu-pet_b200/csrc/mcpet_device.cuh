@@ -136,11 +136,40 @@ __device__ __forceinline__ void emit_first(Rng& r, const TransportParams& P, int
   pos.z = ((float)vz + r3) / P.inv_vz;
 }
 
+/* Direction d turned by the polar angle with cosine c and sine s (s may be
+ * negative: the azimuth turned by pi) around azimuth 2 pi u: the DIRECT
+ * rotation of rotate_fast with the sine given, so that a small angle keeps
+ * its precision. */
+__device__ __forceinline__ void rotate_fast_cs(float3& d, float c, float s, float u) {
+  float sinphi, cosphi;
+  __sincosf(6.28318530717958647693f * u, &sinphi, &cosphi);
+  const float dxy = d.x * d.x + d.y * d.y;
+  if (dxy > 1.0e-14f) {
+    const float sdt = s * rsqrtf(dxy);
+    const float x_in = d.x;
+    d.x = d.x * c + sdt * (x_in * d.z * cosphi - d.y * sinphi);
+    d.y = d.y * c + sdt * (d.y * d.z * cosphi + x_in * sinphi);
+    d.z = d.z * c - dxy * sdt * cosphi;
+  } else {
+    d.y = s * sinphi;
+    if (d.z > 0.0f) {
+      d.x = s * cosphi;
+      d.z = c;
+    } else {
+      d.x = -s * cosphi;
+      d.z = -c;
+    }
+  }
+}
+
 /* Second photon: anti-parallel to the first, tilted by the acolinearity
  * angle theta = 2*0.21276 deg * N(0,1) (Box-Muller, cosine branch) around a
- * uniform azimuth; or isotropic in background mode.  kFast (balanced lanes):
- * the same draws and formulas in single precision instead of the
- * reference's double-precision constants and products. */
+ * uniform azimuth; or isotropic in background mode.  The reference builds it
+ * from the spherical angles of -d1 and a rotation matrix (atan2, acos and
+ * four sincos).  kFast (balanced lanes): the same three draws give theta
+ * and the azimuth, and -d1 is turned by theta directly -- the same
+ * distribution (the azimuth is uniform, so the frame does not matter) for
+ * a fraction of the arithmetic. */
 template <bool kFast = false>
 __device__ __forceinline__ void emit_second(Rng& r, bool background, const float3& d1, float3& d) {
   if (background) {
@@ -149,13 +178,15 @@ __device__ __forceinline__ void emit_second(Rng& r, bool background, const float
   }
   float phi2, theta2, theta_nc, phi_nc;
   if (kFast) {
-    phi2 = atan2f(d1.y, d1.x) + (float)kPi;
-    theta2 = (float)kPi - acosf(d1.z);
     const float v1 = ranecu(r);
     const float v2 = ranecu(r);
     theta_nc = (float)(2.0 * 0.21276 * kPi / 180.0) * sqrtf(-2.0f * __logf(v2 + 1e-8f)) *
                __cosf((float)(2.0 * kPi) * v1);
-    phi_nc = (float)(2.0 * kPi) * ranecu(r);
+    float st, ct;
+    __sincosf(theta_nc, &st, &ct);
+    d = make_float3(-d1.x, -d1.y, -d1.z);
+    rotate_fast_cs(d, ct, st, ranecu(r));
+    return;
   } else {
     phi2 = (float)((double)atan2f(d1.y, d1.x) + kPi);
     theta2 = (float)(kPi - (double)acosf(d1.z));
@@ -499,13 +530,25 @@ __device__ __forceinline__ float to_cylinder(const TransportParams& P, const flo
 /* Sinogram bin of a line of response (MCGPU-PET_kernel.cu:1749-1791) from the
  * azimuths and axial hit positions of the two photons (photon "a" is the one
  * tracked last).  Returns -1 when the pair falls outside the rings, the
- * maximum ring difference or the sinogram. */
+ * maximum ring difference or the sinogram.  kFast (balanced lanes): the
+ * crystal and ring indices in single precision (the reference divides in
+ * double). */
+template <bool kFast = false>
 __device__ __forceinline__ long long sinogram_bin(const TransportParams& P, float phi_a, float z_a,
                                                   float phi_b, float z_b) {
-  int xa = __float2int_rd((float)(((double)phi_a / (2.0 * kPi) + 0.5) * (double)P.ncrystals));
-  int xb = __float2int_rd((float)(((double)phi_b / (2.0 * kPi) + 0.5) * (double)P.ncrystals));
-  int za = __float2int_rd((float)(((double)(z_a / P.fovz) + 0.5) * (double)P.nrows));
-  int zb = __float2int_rd((float)(((double)(z_b / P.fovz) + 0.5) * (double)P.nrows));
+  int xa, xb, za, zb;
+  if (kFast) {
+    const float inv_2pi = (float)(1.0 / (2.0 * kPi)), nc = (float)P.ncrystals, nr = (float)P.nrows;
+    xa = __float2int_rd((phi_a * inv_2pi + 0.5f) * nc);
+    xb = __float2int_rd((phi_b * inv_2pi + 0.5f) * nc);
+    za = __float2int_rd((z_a / P.fovz + 0.5f) * nr);
+    zb = __float2int_rd((z_b / P.fovz + 0.5f) * nr);
+  } else {
+    xa = __float2int_rd((float)(((double)phi_a / (2.0 * kPi) + 0.5) * (double)P.ncrystals));
+    xb = __float2int_rd((float)(((double)phi_b / (2.0 * kPi) + 0.5) * (double)P.ncrystals));
+    za = __float2int_rd((float)(((double)(z_a / P.fovz) + 0.5) * (double)P.nrows));
+    zb = __float2int_rd((float)(((double)(z_b / P.fovz) + 0.5) * (double)P.nrows));
+  }
   if (za < 0 || zb < 0 || za >= P.nrows || zb >= P.nrows) return -1;
   int dz = abs(zb - za);
   if (dz > P.mrd) return -1;
@@ -539,10 +582,13 @@ __device__ __forceinline__ long long sinogram_bin(const TransportParams& P, floa
 }
 
 /* Gaussian energy blur of one photon as drawn by the sinogram tally
- * (MCGPU-PET_kernel.cu:1797-1802): sqrt(-2 ln(u1+1e-8)) cos(2 pi u2). */
+ * (MCGPU-PET_kernel.cu:1797-1802): sqrt(-2 ln(u1+1e-8)) cos(2 pi u2); kFast
+ * (balanced lanes): in single precision. */
+template <bool kFast = false>
 __device__ __forceinline__ float blur_sinogram(Rng& r) {
   float u1 = ranecu(r);
   float u2 = ranecu(r);
+  if (kFast) return sqrtf(-2.0f * __logf(u1 + 1e-8f)) * __cosf((float)(2.0 * kPi) * u2);
   return sqrtf((float)(-2.0 * (double)logf(u1 + 1e-8f))) * cosf((float)((double)(2.0f) * kPi * (double)u2));
 }
 /* ... and as drawn by the PSF tally (MCGPU-PET_kernel.cu:580-585). */

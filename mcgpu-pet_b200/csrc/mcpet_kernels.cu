@@ -117,6 +117,7 @@ __global__ void probe_rayleigh_kernel(RayleighRows R, int n, const float* energy
   seeds[i] = make_int2(r.x, r.y);
 }
 
+template <bool kFast>
 __global__ void probe_source_kernel(TransportParams P, int background, int2* seeds, float3* out) {
   int v = blockIdx.x * blockDim.x + threadIdx.x;
   if ((long long)v >= P.n_voxels) return;
@@ -126,7 +127,7 @@ __global__ void probe_source_kernel(TransportParams P, int background, int2* see
   r.y = seeds[v].y;
   float3 pos, dir, dir2;
   emit_first(r, P, vx, vy, vz, pos, dir);
-  emit_second(r, background != 0, dir, dir2);
+  emit_second<kFast>(r, background != 0, dir, dir2);
   out[4 * v + 0] = pos;
   out[4 * v + 1] = dir;
   out[4 * v + 2] = pos;
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(kBlock) grad_replay_kernel(TransportParams P, 
       to_cylinder(P, a.pos, a.dir, xa, ya, za);
       const float phia = atan2f(ya, xa);
       ok = fabsf(zb) < 0.5f * P.height && fabsf(za) < 0.5f * P.height &&
-           sinogram_bin(P, phib, zb, phia, za) == bin;
+           sinogram_bin<(kMode & kModeFast) != 0>(P, phib, zb, phia, za) == bin;
     }
     if (!ok) {
       ++bad_count;
@@ -668,7 +669,9 @@ cudaError_t launch_probe_rayleigh(const RayleighRows& R, int n, const float* ene
 cudaError_t launch_probe_source(const TransportParams& P, int background, int2* seeds, float3* out,
                                 cudaStream_t s) {
   int n = (int)P.n_voxels;
-  probe_source_kernel<<<(n + 127) / 128, 128, 0, s>>>(P, background, seeds, out);
+  /* bit 0: background mode; bit 1: the balanced lanes' arithmetic */
+  if (background & 2) probe_source_kernel<true><<<(n + 127) / 128, 128, 0, s>>>(P, background & 1, seeds, out);
+  else probe_source_kernel<false><<<(n + 127) / 128, 128, 0, s>>>(P, background & 1, seeds, out);
   return cudaGetLastError();
 }
 

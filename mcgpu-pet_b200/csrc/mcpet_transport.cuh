@@ -263,7 +263,7 @@ __device__ __forceinline__ void put_psf_record(uint32_t* psf, long long k, unsig
  * detector centre (P.cx, P.cy, P.cz).  A spurious pair (a prompt gamma with
  * an annihilation photon) is tallied with the scatter whatever the photons'
  * scatter states. */
-template <bool kCount, bool kRecord = true, bool kPsf = true>
+template <bool kCount, bool kRecord = true, bool kPsf = true, bool kFast = false>
 __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, const float3 centre,
                                             const DeviceTallies& O, int* spec_sh, int voxel,
                                             unsigned long long t_left, const PhotonState& b, const PhotonState& a,
@@ -282,10 +282,10 @@ __device__ __forceinline__ void detect_pair(Rng& rng, const TransportParams& P, 
       to_cylinder(P, centre, a.pos, a.dir, xa, ya, za);
       float phia = atan2f(ya, xa);
       if (fabsf(za) < 0.5f * P.height) {
-        long long bin = sinogram_bin(P, phib, zb, phia, za);
+        long long bin = sinogram_bin<kFast>(P, phib, zb, phia, za);
         if (bin >= 0) {
-          float g1 = blur_sinogram(rng);
-          float g2 = blur_sinogram(rng);
+          float g1 = blur_sinogram<kFast>(rng);
+          float g2 = blur_sinogram<kFast>(rng);
           float eb = b.energy + (P.e_resol / 2.35f) * b.energy * g1;
           float ea = a.energy + (P.e_resol / 2.35f) * a.energy * g2;
           int ib = __float2int_rd(eb / 1000.0f);
@@ -385,6 +385,7 @@ constexpr int kBlock = 256;
 
 template <bool kCount, int kMode>
 __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, DeviceTables T, DeviceTallies O) {
+  constexpr bool kFastLanes = (kMode & kModeFast) != 0;
   __shared__ ComptonTable cmp;
   __shared__ unsigned long long mdose_sh[2 * kMaxMaterials];
   if (threadIdx.x < 2 * kMaxMaterials) mdose_sh[threadIdx.x] = 0;
@@ -465,8 +466,8 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
         bool pass = (P.tally_type == 0) || (P.tally_type == 1 && b.state == 0 && a.state == 0) ||
                     (P.tally_type == 2 && (b.state != 0 || a.state != 0));
         if (pass)
-          detect_pair<kCount>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel, t_left, b, a, cnt, detected,
-                              rng_emit);
+          detect_pair<kCount, true, true, kFastLanes>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel,
+                                                      t_left, b, a, cnt, detected, rng_emit);
       }
       /* prompt gamma: isotropic from the decay point after the pair, then
        * its pairs with the annihilation photons that escaped (spurious
@@ -484,11 +485,11 @@ __global__ void __launch_bounds__(kBlock) transport_kernel(TransportParams P, De
                                                        dose_on ? &dose : nullptr);
         if (esc_g && P.tally_type != 1) {
           if (esc_a)
-            detect_pair<kCount>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel, t_left, g, a, cnt,
-                                detected, rng_emit, true);
+            detect_pair<kCount, true, true, kFastLanes>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel,
+                                                        t_left, g, a, cnt, detected, rng_emit, true);
           if (esc_b)
-            detect_pair<kCount>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel, t_left, g, b, cnt,
-                                detected, rng_emit, true);
+            detect_pair<kCount, true, true, kFastLanes>(rng, P, make_float3(P.cx, P.cy, P.cz), O, spec_sh, voxel,
+                                                        t_left, g, b, cnt, detected, rng_emit, true);
         }
       }
     }
@@ -870,7 +871,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
                                                (PD.tally_type == 2 && (ph.state != 0 || a.state != 0));
               if (pass) {
                 unsigned long long det = 0;
-                detect_pair<kCount, kRecord, !(kMode & kModeSino)>(rng, PD, make_float3(PD.cx, PD.cy, PD.cz),
+                detect_pair<kCount, kRecord, !(kMode & kModeSino), (kMode & kModeFast) != 0>(rng, PD, make_float3(PD.cx, PD.cy, PD.cz),
                                                                   kBatch ? slots[scene].O : O,
                                              spec_sh, (int)cold.u(kCVox),
                                              cold.t_left(), ph, a, cnt, det,

@@ -599,11 +599,14 @@ def probe_rayleigh(scene: Scene, energy, mat, pmax, seeds):
     return c_out, s_out
 
 
-def probe_source(shape, inv_voxel_size, seeds, background: bool = False):
+def probe_source(shape, inv_voxel_size, seeds, background: bool = False, balanced: bool = False):
+    """Photon pairs of every voxel (mcpet_probe_source); balanced: the
+    balanced lanes' photon-2 emission."""
     nz, ny, nx = shape
     inv = np.ascontiguousarray(inv_voxel_size, np.float32)
     s = np.ascontiguousarray(seeds, np.int32).reshape(-1, 2)
     out = np.zeros((nx * ny * nz, 4, 3), np.float32)
     s_out = np.zeros_like(s)
-    check(lib().mcpet_probe_source(nx, ny, nz, _ptr(inv), int(bool(background)), _ptr(s), _ptr(out), _ptr(s_out)))
+    mode = int(bool(background)) | (2 if balanced else 0)
+    check(lib().mcpet_probe_source(nx, ny, nz, _ptr(inv), mode, _ptr(s), _ptr(out), _ptr(s_out)))
     return out, s_out

@@ -61,6 +61,42 @@ def test_source_bit_exact_vs_reference_device_code(background):
         assert np.array_equal(_u8(a), _u8(b)) and np.array_equal(sa, sb)
 
 
+def test_balanced_photon2_emission_has_the_reference_distribution():
+    """Balanced lanes turn -d1 by the acolinearity angle directly instead of
+    through spherical angles and a rotation matrix: same first photon (same
+    draws, same code), and the angle between photon 2 and -d1 and its
+    azimuth around -d1 follow the reference form's distributions (two-sample
+    Kolmogorov-Smirnov on 2.6e5 pairs), with theta = 2 * 0.21276 deg * |N(0,1)|."""
+    stats = pytest.importorskip("scipy.stats")
+    shape = (64, 64, 64)
+    inv = (1.0, 1.0, 1.0)
+    seeds, _, _ = mcpet.probe_rng(4321, np.arange(np.prod(shape)), 0)
+    ref, s_ref = mcpet.probe_source(shape, inv, seeds)
+    fast, s_fast = mcpet.probe_source(shape, inv, seeds, balanced=True)
+    np.testing.assert_array_equal(ref[:, :3], fast[:, :3])      # photon 1 and photon 2's start point
+    np.testing.assert_array_equal(s_ref, s_fast)                # three draws either way
+
+    def angles(out):
+        d1, d2 = out[:, 1].astype(np.float64), out[:, 3].astype(np.float64)
+        n = -d1 / np.linalg.norm(d1, axis=1, keepdims=True)
+        theta = np.arccos(np.clip(np.sum(d2 * n, axis=1) / np.linalg.norm(d2, axis=1), -1.0, 1.0))
+        axis = np.where(np.abs(n[:, 2:3]) < 0.9, [[0.0, 0.0, 1.0]], [[1.0, 0.0, 0.0]])
+        e1 = np.cross(n, axis)
+        e1 /= np.linalg.norm(e1, axis=1, keepdims=True)
+        e2 = np.cross(n, e1)
+        phi = np.arctan2(np.sum(d2 * e2, axis=1), np.sum(d2 * e1, axis=1))
+        return theta, phi, np.linalg.norm(d2, axis=1)
+
+    t_r, p_r, n_r = angles(ref)
+    t_f, p_f, n_f = angles(fast)
+    assert np.all(np.abs(n_f - 1.0) < 1e-5) and np.all(np.abs(n_r - 1.0) < 1e-5)
+    sigma = 2.0 * 0.21276 * np.pi / 180.0
+    assert abs(np.sqrt(np.mean(t_f ** 2)) / sigma - 1.0) < 0.01
+    assert stats.ks_2samp(t_r, t_f).pvalue > 1e-3
+    assert stats.ks_2samp(p_r, p_f).pvalue > 1e-3
+    assert stats.kstest((p_f + np.pi) / (2 * np.pi), "uniform").pvalue > 1e-3
+
+
 @needs_ref_gpu
 def test_compton_rayleigh_bit_exact_vs_reference_device_code(sample):
     t = sample.export_tables()
