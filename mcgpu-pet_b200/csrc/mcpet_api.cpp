@@ -824,14 +824,17 @@ mcpet_status check_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
 
 /* One launch of a batched run: a range of slots, its launch-wide
  * parameters and tables, and its shape.  A scene with enough decays and
- * lanes to fill the GPU by itself is a launch of its own ("solo": its own
- * tables, no lookup of the scene per lane); the other scenes share one. */
+ * lanes to fill the GPU by itself is a launch of its own ("solo"): the
+ * single-scene kernel of a run of it alone, with its parameters, tables and
+ * tallies; the other scenes share one launch of the batch kernel. */
 struct BatchGroup {
   int first = 0, count = 0;         /* slots [first, first + count) */
   TransportParams P;                /* launch-wide parameters (the group's lanes) */
   DeviceTables T;
+  DeviceTallies O;                  /* solo: the scene's tallies */
   int share = 0;                    /* kBatchShareScanner | kBatchSharePhantom */
   bool solo = false;
+  int mode = 0, algorithm = 0;      /* solo: kernel variant of the scene's own run */
   int grid = 1;
   size_t smem = 0;
 };
@@ -855,7 +858,8 @@ struct BatchLaunch {
 };
 
 /* A scene of at least this many decays runs as a launch of its own when its
- * lanes fill the GPU twice over. */
+ * lanes fill the GPU twice over (runs without counters, dose tallies or a
+ * prompt gamma: the chained variant is the plain event kernel). */
 constexpr double kSoloDecays = 2.0e7;
 
 /* Decays of a scene's full acquisition (also while the autotuner runs it on
@@ -901,6 +905,7 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   int max_shells = 1;
   L.total = 0;
   std::vector<char> solo((size_t)n, 0);
+  std::vector<TransportParams> alone((size_t)n);   /* each scene's parameters as in a run of it alone */
   for (int k = 0; k < n; ++k) {
     mcpet_scene* sc = scenes[k];
     sc->dev.run_h2d = 0;
@@ -920,12 +925,17 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
     s = build_lanes(sc, o.lane_mode, tpb, hpl, st);
     if (s != MCPET_OK) return s;
     const double resident = (double)std::max(sc->dev.sm_count, 1) * 2048.0;
-    solo[(size_t)k] = scene_decays(sc) >= kSoloDecays && (double)sc->dev.n_lanes >= 2.0 * resident;
+    const bool plain = !(o.collect_counters && outs[0].counters) && !outs[k].mat_dose && !outs[k].vox_dose &&
+                       !(run_mode(sc, o) & kTransportPrompt);
+    solo[(size_t)k] = plain && scene_decays(sc) >= kSoloDecays && (double)sc->dev.n_lanes >= 2.0 * resident;
     SceneSlot& z = L.slots[(size_t)k];
     memset(&z, 0, sizeof(z));
     z.O = outs[k];
     s = prepare_params(sc, o, z.O, z.P);
     if (s != MCPET_OK) return s;
+    alone[(size_t)k] = z.P;
+    alone[(size_t)k].n_lanes = sc->dev.n_lanes;
+    alone[(size_t)k].n_emitters = sc->dev.n_emitters;
     z.P.spectrum_in_shared = 0;
     z.P.palette_in_shared = 0;
     z.P.n_lanes = sc->dev.n_lanes;
@@ -971,6 +981,17 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
       lanes += L.slots[(size_t)i].P.n_lanes;
     }
     L.total += lanes;
+    if (g.solo) {
+      const int k = L.scene_of[(size_t)j];
+      g.P = alone[(size_t)k];
+      g.T = L.slots[(size_t)j].T;
+      g.O = L.slots[(size_t)j].O;
+      g.mode = run_mode(scenes[k], o) | kTransportChained;
+      g.algorithm = kAlgorithmEvents;
+      L.groups.push_back(g);
+      j += g.count;
+      continue;
+    }
     g.P = L.slots[(size_t)j].P;
     g.P.n_lanes = lanes;
     g.P.n_emitters = 0;
@@ -1005,6 +1026,15 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
   L.mode = (o.lane_mode == MCPET_LANES_BALANCED ? kTransportFast : 0) | (prompt ? kTransportPrompt : 0) |
            (sino_only ? kTransportSinogramOnly : 0);
   for (BatchGroup& g : L.groups) {
+    if (g.solo) {
+      g.smem = transport_dynamic_smem(g.P, L.block, g.algorithm);
+      int bps = 0;
+      CUDA_TRY(transport_occupancy(L.counters, g.algorithm, g.mode, L.block, g.smem, &bps));
+      if (bps < 1) return set_error(MCPET_ERR_LIMIT, "transport kernel does not fit on an SM (smem %zu)", g.smem);
+      if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
+      g.grid = g.P.n_lanes == 0 ? 1 : s0->dev.sm_count * bps;
+      continue;
+    }
     g.share = 0;
     if (!L.counters && !L.dose) {
       bool scanner = true, phantom = true;
@@ -1079,13 +1109,21 @@ mcpet_status enqueue_batch_launch(mcpet_scene* const* scenes, int n, BatchLaunch
   if (ev0) CUDA_TRY(cudaEventRecord(ev0, st));
   for (size_t i = 0; i < L.groups.size(); ++i) {
     const BatchGroup& g = L.groups[i];
+    const SceneSlot* slots = reinterpret_cast<const SceneSlot*>(dbuf) + g.first;
     DeviceTallies O;
     memset(&O, 0, sizeof(O));
+    if (g.solo) {
+      O = g.O;
+      O.seed_word = &slots->P.seed;   /* the slot's seed: graph replays advance it */
+    }
     O.guard = guard;
     O.lane_cursor = cursors + i;
     O.counters = L.counter_words;
-    CUDA_TRY(launch_transport_batch(g.P, g.T, O, reinterpret_cast<const SceneSlot*>(dbuf) + g.first, g.count,
-                                    L.counters, L.dose, g.share, L.mode, g.grid, L.block, g.smem, i > 0, st));
+    if (g.solo)
+      CUDA_TRY(launch_transport(g.P, g.T, O, L.counters, g.algorithm, g.mode, g.grid, L.block, g.smem, st, i > 0));
+    else
+      CUDA_TRY(launch_transport_batch(g.P, g.T, O, slots, g.count, L.counters, L.dose, g.share, L.mode, g.grid,
+                                      L.block, g.smem, i > 0, st));
   }
   if (ev1) CUDA_TRY(cudaEventRecord(ev1, st));
   return MCPET_OK;
@@ -1629,6 +1667,8 @@ mcpet_status mcpet_batch_graph_create(mcpet_scene* const* scenes, int n_scenes, 
     L.slots[(size_t)L.slot_of[(size_t)k]].T.emitters = g->plans + off;
     off += (size_t)d.n_emitters;
   }
+  for (BatchGroup& grp : L.groups)
+    if (grp.solo) grp.T.emitters = L.slots[(size_t)grp.first].T.emitters;
   CUDA_TRY(cudaMalloc((void**)&g->dbuf, L.bytes));
   const std::vector<unsigned char> host = batch_blob(L);
   CUDA_TRY(cudaMemcpy(g->dbuf, host.data(), L.bytes, cudaMemcpyHostToDevice));

@@ -21,13 +21,16 @@ constexpr int kTransportFast = 1;
 constexpr int kTransportPrompt = 2;
 constexpr int kTransportCaps = 4;
 constexpr int kTransportSinogramOnly = 8;   /* no PSF tally (and no sinogram-dry PSF replays) */
+constexpr int kTransportChained = 16;       /* single-scene launch of a batched run that may follow another
+                                               (programmatic dependent launch; seed read from the batch
+                                               slot); plain event kernel, modes 0, 1, 8, 9 only */
 
 size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();
 cudaError_t transport_occupancy(bool counters, int algorithm, int mode, int block, size_t smem, int* blocks_per_sm);
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int mode, int grid, int block, size_t smem,
-                             cudaStream_t stream);
+                             cudaStream_t stream, bool after_previous = false);
 
 /* batched runs: several scenes in one launch of the event kernel.  share:
  * bit 0 = every scene has the launch's scanner (detector, sinogram, tally

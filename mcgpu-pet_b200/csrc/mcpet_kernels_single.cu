@@ -10,8 +10,20 @@ using namespace dev;
 
 namespace {
 
+/* Chained single-scene launches of a batched run (plain event kernel). */
+EventKernel chained_event_kernel(int mode) {
+  switch (mode) {
+    case kTransportChained | 0: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 16>;
+    case kTransportChained | 1: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 17>;
+    case kTransportChained | 8: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 24>;
+    case kTransportChained | 9: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 25>;
+    default: return nullptr;
+  }
+}
+
 /* Single-scene transport kernel of a run: algorithm, counters, mode. */
 EventKernel single_event_kernel(bool counters, int algorithm, int mode) {
+  if (mode & kTransportChained) return (!counters && algorithm == kAlgorithmEvents) ? chained_event_kernel(mode) : nullptr;
   if (algorithm == kAlgorithmEventsDose)
     return counters ? event_variant<true, kEventBlocks, false, false, false, true, 0, 11>(mode)
                     : event_variant<false, kEventBlocks, false, false, false, true, 0, 11>(mode);
@@ -52,15 +64,34 @@ cudaError_t transport_occupancy(bool counters, int algorithm, int mode, int bloc
 
 cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, const DeviceTallies& O,
                              bool counters, int algorithm, int mode, int grid, int block, size_t smem,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, bool after_previous) {
   if (algorithm == kAlgorithmHistories) {
+    if (after_previous) return cudaErrorNotSupported;
     HistoryKernel k = counters ? history_variant<true>(mode) : history_variant<false>(mode);
     k<<<grid, block, smem, stream>>>(P, T, O);
     return cudaGetLastError();
   }
   EventKernel k = single_event_kernel(counters, algorithm, mode);
   if (!k) return cudaErrorNotSupported;
-  k<<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
+  if (!after_previous) {
+    k<<<grid, block, smem, stream>>>(P, T, O, nullptr, 0);
+    return cudaGetLastError();
+  }
+  /* a launch of a batched run after another: it may start placing blocks
+   * while the previous one drains (programmatic dependent launch) */
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const SceneSlot* none = nullptr;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, k, P, T, O, none, 0);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

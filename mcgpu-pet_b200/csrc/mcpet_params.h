@@ -142,6 +142,8 @@ struct DeviceTallies {
   uint32_t* events;               /* detected-coincidence records (EventRecord) for the gradient, or NULL */
   unsigned long long* event_count;
   long long event_capacity;
+  const int* seed_word;           /* RANECU seed on the device (a batch's slot, advanced by graph
+                                     replays), or NULL: P.seed */
 };
 
 /* One tallied coincidence, enough to replay its history: the lane's RANECU

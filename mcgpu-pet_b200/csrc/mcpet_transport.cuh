@@ -38,7 +38,7 @@ struct LaneCounters {
  * tally the sinogram only.  A variant carries none of the code of the
  * features it leaves out. */
 constexpr int kModeFast = kTransportFast, kModePrompt = kTransportPrompt, kModeCaps = kTransportCaps,
-              kModeSino = kTransportSinogramOnly;
+              kModeSino = kTransportSinogramOnly, kModeChain = kTransportChained;
 
 template <int kMode>
 __device__ __forceinline__ int steps_cap(const TransportParams& P) {
@@ -924,7 +924,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
             const Emitter* em = plan + find_emitter(plan, plan_n, local);
             const TransportParams& PN = kBatch ? slots[scene].P : P;
             /* the jump tables are the same for every scene: the launch's */
-            rng = rng_stream(P, PN.seed, __ldg(&em->stream_base) + (local - __ldg(&em->first_lane)));
+            const int seed = (!kBatch && (kMode & kModeChain)) ? __ldg(O.seed_word) : PN.seed;
+            rng = rng_stream(P, seed, __ldg(&em->stream_base) + (local - __ldg(&em->first_lane)));
             cold.set_inv_rate(__ldg(&em->inv_rate));
             cold.set_t_left(PN.acq_ps);
             cold.u(kCVox) = __ldg(&em->voxel);
@@ -1044,8 +1045,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
   }
 
   /* a batched run's next launch may start placing its blocks as this
-   * grid's blocks run out of lanes (programmatic dependent launch) */
-  if (kBatch) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+   * grid's blocks run out of lanes (programmatic dependent launch; no effect
+   * on a launch without that dependency) */
+  if (kBatch || (kMode & kModeChain)) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (kBatch) {
     flush_lane();
   } else {
@@ -1075,7 +1077,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
    * blocks are resident or done once this grid runs), so the stream's later
    * work sees every launch of the run finished; a no-op without a
    * programmatic dependency */
-  if (kBatch) asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (kBatch || (kMode & kModeChain)) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 /* ---------------------------------------------------------- launch helpers */
