@@ -244,10 +244,16 @@ def measure_reference_cuda(workdir: str, emissions: float) -> dict:
                     "kernel time from CUDA events on this GPU"}
 
 
+PROMPT_GAMMA_EV = 1157020.0   # the prompt gamma of the batched workload's second emitter
+
+
 def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, replays: int = 3) -> dict:
-    """Batched many-phantom workload (config C3 shapes): n_scenes head-like
-    phantoms of uneven size, each its own seed.  Device-resident tallies
-    throughout; times are CUDA events on the launch stream.
+    """Batched many-phantom workload (config C3): n_scenes head-like phantoms
+    of uneven size, each its own seed; the even ones a pure 511 keV positron
+    emitter, the odd ones an emitter with a 1157 keV prompt gamma at 100 %
+    yield (every scene on the material tables continued to 1250 keV, which
+    leave 511 keV results unchanged).  Device-resident tallies throughout;
+    times are CUDA events on the launch stream.
 
     * sequential: the scenes one after another through mcpet_run_device
       (one launch each), the plain form of the run;
@@ -262,8 +268,11 @@ def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, re
     from mcpet import inputs
     sc, sizes = [], []
     for k, (mat, rho, act, vs, used) in enumerate(inputs.batch_phantoms(n_scenes, emissions_each)):
-        spec = inputs.spec_for(inputs.tissue_materials(list(inputs.TISSUES)[:8]), "unused.vox", seed=1000 + k,
-                               **inputs.scanner_batch())
+        kw = dict(inputs.scanner_batch(), seed=1000 + k)
+        if k % 2:
+            kw.update(prompt_gamma_energy=PROMPT_GAMMA_EV, prompt_gamma_yield=1.0)
+        spec = inputs.spec_for(inputs.tissue_materials(list(inputs.TISSUES)[:8], extended=True), "unused.vox",
+                               **kw)
         cfg = inputs.config_from_spec(spec, workdir)
         sc.append(mcpet.Scene.from_arrays(cfg, mat, rho, act, vs))
         sizes.append(mat.shape[0])
@@ -324,8 +333,9 @@ def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, re
         s.close()
     rate = lambda c, ms: c / (ms * 1e-3)
     return {"workload": f"{n_scenes} head-like phantoms of m^3 voxels, m in [32,192] (min {min(sizes)}, max "
-                        f"{max(sizes)}), 2-4 mm voxels, {emissions_each:.0e} decays each, own seed each; scanner "
-                        "32 rings, 128 rad x 128 ang x 1985 planes (span 1); device-resident tallies",
+                        f"{max(sizes)}), 2-4 mm voxels, {emissions_each:.0e} decays each, own seed each; half "
+                        "pure 511 keV emitters, half with a 1157 keV prompt gamma at 100 % yield (tables to 1250 "
+                        "keV); scanner 32 rings, 128 rad x 128 ang x 1985 planes (span 1); device-resident tallies",
             "unit": UNIT, "tuned_batch_identical_to_tuned_sequential": identical,
             "sequential": {"ms": seq_ms, "wall_s": seq_wall, "value": rate(seq_c, seq_ms), "launches": n_scenes},
             "batched": {"ms": bat_ms, "wall_s": bat_wall, "value": rate(bat_c, bat_ms), "launches": 1},

@@ -260,8 +260,8 @@ mcpet_status mcpet_run_device(mcpet_scene* scene, const mcpet_run_opts* opts,
  * histories per lane, <= 0, every scene gets its own automatic lanes).  A
  * scene of at least 2e7 decays whose lanes fill the GPU twice over runs as
  * a launch of its own -- the single-scene kernel of a run of it alone, when
- * the batch collects no counters and the scene tallies no dose and emits no
- * prompt gamma; the other scenes share one launch of the batch kernel.  The launches follow one another on the stream, each allowed to
+ * the batch collects no counters and the scene tallies no dose; the other
+ * scenes share one launch of the batch kernel.  The launches follow one another on the stream, each allowed to
  * start placing blocks (programmatic dependent launch) while the previous
  * one drains its last lanes.  The scenes must use the same material files
  * in the same slots (the shared launch reads one Compton and Rayleigh table

@@ -858,8 +858,8 @@ struct BatchLaunch {
 };
 
 /* A scene of at least this many decays runs as a launch of its own when its
- * lanes fill the GPU twice over (runs without counters, dose tallies or a
- * prompt gamma: the chained variant is the plain event kernel). */
+ * lanes fill the GPU twice over (runs without counters or dose tallies: the
+ * chained variant is the plain event kernel). */
 constexpr double kSoloDecays = 2.0e7;
 
 /* Decays of a scene's full acquisition (also while the autotuner runs it on
@@ -925,8 +925,7 @@ mcpet_status setup_batch(mcpet_scene* const* scenes, int n, const mcpet_run_opts
     s = build_lanes(sc, o.lane_mode, tpb, hpl, st);
     if (s != MCPET_OK) return s;
     const double resident = (double)std::max(sc->dev.sm_count, 1) * 2048.0;
-    const bool plain = !(o.collect_counters && outs[0].counters) && !outs[k].mat_dose && !outs[k].vox_dose &&
-                       !(run_mode(sc, o) & kTransportPrompt);
+    const bool plain = !(o.collect_counters && outs[0].counters) && !outs[k].mat_dose && !outs[k].vox_dose;
     solo[(size_t)k] = plain && scene_decays(sc) >= kSoloDecays && (double)sc->dev.n_lanes >= 2.0 * resident;
     SceneSlot& z = L.slots[(size_t)k];
     memset(&z, 0, sizeof(z));

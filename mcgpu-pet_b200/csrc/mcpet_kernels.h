@@ -23,7 +23,7 @@ constexpr int kTransportCaps = 4;
 constexpr int kTransportSinogramOnly = 8;   /* no PSF tally (and no sinogram-dry PSF replays) */
 constexpr int kTransportChained = 16;       /* single-scene launch of a batched run that may follow another
                                                (programmatic dependent launch; seed read from the batch
-                                               slot); plain event kernel, modes 0, 1, 8, 9 only */
+                                               slot); plain event kernel, no loop caps */
 
 size_t transport_dynamic_smem(const TransportParams& P, int block, int algorithm);
 int transport_block_threads();

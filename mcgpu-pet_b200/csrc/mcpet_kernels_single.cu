@@ -17,6 +17,10 @@ EventKernel chained_event_kernel(int mode) {
     case kTransportChained | 1: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 17>;
     case kTransportChained | 8: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 24>;
     case kTransportChained | 9: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 25>;
+    case kTransportChained | 2: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 18>;
+    case kTransportChained | 3: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 19>;
+    case kTransportChained | 10: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 26>;
+    case kTransportChained | 11: return transport_events_kernel<false, kEventBlocks, false, false, false, false, 0, 27>;
     default: return nullptr;
   }
 }

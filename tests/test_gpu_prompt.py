@@ -133,3 +133,26 @@ def test_batch_mixing_prompt_and_pure_emitters_equals_runs_alone(workdir):
     assert scs[0].guard_trips() == 0
     for s in scs:
         s.close()
+
+
+def test_batch_with_a_large_prompt_scene_in_its_own_launch(workdir):
+    """A prompt-gamma head of 2.5e7 decays runs as a chained launch of its
+    own (the single-scene kernel's prompt variant), the small scenes share
+    the batch launch: every scene equals its run alone (automatic lanes)."""
+    mat, rho, act, vs, _ = inputs.head_phantom(shape=(40, 64, 64), voxel_cm=0.4, seed=21, total_bq=2.5e7)
+    big = scenes.scene_from_arrays(workdir, mat, rho, act, vs, tissues=list(inputs.TISSUES)[:8], extended=True,
+                                   seed=31, prompt_gamma_energy=PROMPT_EV, **inputs.scanner_batch())
+    scs = [big]
+    for k, (m, r, a, v, used) in enumerate(inputs.batch_phantoms(2, 2.0e5, seed=5)):
+        scs.append(scenes.scene_from_arrays(workdir, m, r, a, v, tissues=list(inputs.TISSUES)[:8], extended=True,
+                                            seed=600 + k, **inputs.scanner_batch()))
+    opts = mcpet.RunOptions(lane_mode=mcpet.LANES_BALANCED)
+    alone = [s.run(opts) for s in scs]
+    batch = mcpet.Scene.run_batch(scs, opts)
+    for k, (a, b) in enumerate(zip(alone, batch)):
+        for key in ("trues", "scatter", "image_trues", "image_scatter", "spectrum"):
+            np.testing.assert_array_equal(getattr(a, key), getattr(b, key), err_msg=f"scene {k}: {key}")
+        assert a.total_histories == b.total_histories and a.detected == b.detected
+    assert alone[0].total_histories > 2 * 2.4e7     # three photons per decay
+    for s in scs:
+        s.close()
