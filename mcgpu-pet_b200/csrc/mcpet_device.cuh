@@ -380,8 +380,10 @@ __device__ __forceinline__ float compton_s0(float E, int mat, const ComptonTable
  * Returns true on acceptance, with tau, cdt1 = 1 - cos(theta), the sum s and
  * the shell terms rn[] that the second stage reads.  A trial draws the same
  * random numbers whether the trials of one sampling run back to back or
- * with other work of the thread between them. */
-template <typename Scratch>
+ * with other work of the thread between them.  kFast (balanced lanes): the
+ * envelope branch and cdt1 in single precision instead of the reference's
+ * double-precision constant and division. */
+template <bool kFast = false, typename Scratch>
 __device__ __forceinline__ bool compton_trial(Rng& r, float E, int mat, const ComptonTable& C, Scratch rn,
                                               float s0, float& tau, float& s, double& cdt1) {
   const int nsh = C.noscco[mat];
@@ -390,13 +392,21 @@ __device__ __forceinline__ bool compton_trial(Rng& r, float E, int mat, const Co
   float ek3 = ek * ek;
   float taumin = 1.f / ek2;
   float a1 = logf(ek2);
-  if (ranecu(r) * (a1 + 2. * ek * (ek + 1.f) * taumin * taumin) < a1) {
+  const bool first_branch = kFast ? (ranecu(r) * (a1 + 2.f * ek * (ek + 1.f) * taumin * taumin) < a1)
+                                   : (ranecu(r) * (a1 + 2. * ek * (ek + 1.f) * taumin * taumin) < a1);
+  if (first_branch) {
     tau = powf(taumin, ranecu(r));
   } else {
     tau = sqrtf(1.f + ranecu(r) * (taumin * taumin - 1.f));
   }
-  cdt1 = (double)(1.f - tau) / (((double)tau) * ((double)E) * 1.956951306108245e-6);
-  if (cdt1 > 2.0) cdt1 = 1.99999999;
+  if (kFast) {
+    float c = (1.f - tau) / (tau * ek);
+    if (c > 2.0f) c = 1.99999999f;
+    cdt1 = c;
+  } else {
+    cdt1 = (double)(1.f - tau) / (((double)tau) * ((double)E) * 1.956951306108245e-6);
+    if (cdt1 > 2.0) cdt1 = 1.99999999;
+  }
   s = 0.0f;
   for (int i = 0; i < nsh; ++i) {
     float u = C.uico[mat + i * kMaxMaterials];
@@ -427,8 +437,9 @@ __device__ __forceinline__ bool compton_trial(Rng& r, float E, int mat, const Co
 /* GCOa's second stage after an accepted trial (MCGPU-PET_kernel.cu:1453-1562):
  * the target shell and projected momentum pz with the F(EP) rejection, then
  * the energy of the scattered photon.  costh = 1 - cdt1 of the trial.
- * Returns false when the rejection guard fired. */
-template <typename Scratch>
+ * Returns false when the rejection guard fired.  kFast (balanced lanes):
+ * the angle term in single precision (the reference's mixes in double). */
+template <bool kFast = false, typename Scratch>
 __device__ __forceinline__ bool compton_doppler(Rng& r, float& energy, int mat, const ComptonTable& C, Scratch rn,
                                                 float tau, float s, double costh,
                                                 int max_rejections = kMaxRejections) {
@@ -456,7 +467,7 @@ __device__ __forceinline__ bool compton_doppler(Rng& r, float& energy, int mat, 
               (C.fj0[mat + ish * kMaxMaterials] * 1.4142135623731f);
     }
     if (pzomc < -1.0f) continue;
-    t = tau * (tau - costh * 2.f) + 1.f;
+    t = kFast ? tau * (tau - (float)costh * 2.f) + 1.f : tau * (tau - costh * 2.f) + 1.f;
     if (t > 1.0e-20f) {
       af = sqrtf(t) * (tau * (tau - ((float)costh)) / t + 1.f);
     } else {
@@ -486,7 +497,7 @@ __device__ __forceinline__ bool compton_doppler(Rng& r, float& energy, int mat, 
 /* The whole sampling: trials until one is accepted, then the second stage.
  * s0 < 0: the normaliser evaluated at the photon's energy (the reference's
  * arithmetic); else the bound given (MfpRecord::s0_bound). */
-template <typename Scratch>
+template <bool kFast = false, typename Scratch>
 __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, const ComptonTable& C,
                                                Scratch rn, double& costh, float s0_given = -1.0f,
                                                int max_rejections = kMaxRejections) {
@@ -497,10 +508,10 @@ __device__ __forceinline__ bool sample_compton(Rng& r, float& energy, int mat, c
   int it = 0;
   for (;;) {
     if (++it > max_rejections) return false;
-    if (compton_trial(r, E, mat, C, rn, s0, tau, s, cdt1)) break;
+    if (compton_trial<kFast>(r, E, mat, C, rn, s0, tau, s, cdt1)) break;
   }
   costh = 1.0 - cdt1;
-  return compton_doppler(r, energy, mat, C, rn, tau, s, costh, max_rejections);
+  return compton_doppler<kFast>(r, energy, mat, C, rn, tau, s, costh, max_rejections);
 }
 
 /* ------------------------------------------------------------------------

@@ -194,8 +194,9 @@ __device__ __forceinline__ bool track_photon(Rng& rng, const TransportParams& P,
       /* Compton */
       double costh;
       const float e_before = energy;
-      if (!sample_compton(rng, energy, mat0, C, rn, costh, (kMode & kModeFast) ? rec_hi.w : -1.0f,
-                          rejections_cap<kMode>(P))) {
+      if (!sample_compton<(kMode & kModeFast) != 0>(rng, energy, mat0, C, rn, costh,
+                                                    (kMode & kModeFast) ? rec_hi.w : -1.0f,
+                                                    rejections_cap<kMode>(P))) {
         Counting<true>::add(cnt.guard, 1);
         ph.energy = energy;
         return false;
@@ -765,14 +766,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) transport_events_kernel(Tr
           for (;;) {
             if (!accepted && !tripped) {
               if (++trials > (uint32_t)rejections_cap<kMode>(P)) tripped = true;
-              else accepted = compton_trial(rng, e, mat0, cmp, rn, s0, tau, s, cdt1);
+              else accepted = compton_trial<(kMode & kModeFast) != 0>(rng, e, mat0, cmp, rn, s0, tau, s, cdt1);
             }
             if (8 * __popc(__ballot_sync(m_c, !accepted && !tripped)) <= __popc(m_c)) break;
           }
           if (accepted) {
             cold.u(kCTrial) = 0;
             costh = 1.0 - cdt1;
-            ok = compton_doppler(rng, e, mat0, cmp, rn, tau, s, costh, rejections_cap<kMode>(P));
+            ok = compton_doppler<(kMode & kModeFast) != 0>(rng, e, mat0, cmp, rn, tau, s, costh,
+                                                           rejections_cap<kMode>(P));
           } else if (tripped) {
             cold.u(kCTrial) = 0;
           } else {
