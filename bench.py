@@ -257,7 +257,8 @@ def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, re
 
     * sequential: the scenes one after another through mcpet_run_device
       (one launch each), the plain form of the run;
-    * batched: one mcpet_run_batch_device launch over all scenes;
+    * batched: one mcpet_run_batch_device call over all scenes (small
+      scenes share a launch, large ones get chained launches of their own);
     * autotuned: mcpet_autotune picks histories per lane and block size on a
       sample, then the batched launch with that choice;
     * graph: the tuned batch captured once (mcpet_batch_graph_create) and
@@ -398,7 +399,7 @@ def measure_beds(n_beds: int, workdir: str, emissions_total: float = 5.0e9) -> d
     at 2 mm with 10 tissues (lungs, bone, hot organ at 8x), 1 m scanner of
     256 rings, 384 x 384 x 12333-plane span-11 sinograms (1.82e9 bins, int32),
     n_beds bed positions 20 cm apart sharing emissions_total decays.  The beds
-    run batched in one launch and one by one (mcpet_run_batch_device vs
+    run batched and one by one (mcpet_run_batch_device vs
     mcpet_run_device, device-resident tallies, CUDA events); then the
     activity and density-scale gradient of one bed's sinogram
     log-likelihood (mcpet_grad) against a plain forward of that bed."""

@@ -32,7 +32,7 @@ cudaError_t launch_transport(const TransportParams& P, const DeviceTables& T, co
                              bool counters, int algorithm, int mode, int grid, int block, size_t smem,
                              cudaStream_t stream, bool after_previous = false);
 
-/* batched runs: several scenes in one launch of the event kernel.  share:
+/* batched runs: several scenes in one launch of the batch event kernel.  share:
  * bit 0 = every scene has the launch's scanner (detector, sinogram, tally
  * settings), bit 1 = every scene has the launch's phantom (grid, voxel keys,
  * palette, tables); those are then read from P and T (non-counting,

@@ -397,10 +397,11 @@ class Scene:
     @staticmethod
     def run_batch(scenes: list, opts: Optional[RunOptions] = None,
                   psf_capacity: Optional[int] = None) -> list:
-        """Several scenes in one launch (mcpet_run_batch); one RunResult per
-        scene, each equal to scene.run(opts) on its own.  transport_ms is the
-        time of the whole launch; counters (if requested) are launch totals
-        reported on the first result."""
+        """Several scenes in one batched run (mcpet_run_batch: small scenes in
+        one launch, large ones in chained launches of their own); one
+        RunResult per scene, each equal to scene.run(opts) on its own.
+        transport_ms is the time of all the launches; counters (if requested)
+        are their totals, reported on the first result."""
         opts = opts or RunOptions()
         hs = [sc._host_run(psf_capacity) for sc in scenes]
         arr = (_abi.Tallies * len(hs))(*[h.t for h in hs])
@@ -511,9 +512,9 @@ class Scene:
     @staticmethod
     def run_batch_device(scenes: list, tallies: list, opts: Optional[RunOptions] = None,
                          time_it: bool = False) -> float:
-        """Several scenes in one launch into device tallies
+        """Several scenes in one batched run into device tallies
         (mcpet_run_batch_device); ``tallies[k]`` as for run_device.  Returns
-        the launch's transport time in ms when ``time_it``."""
+        the run's transport time in ms when ``time_it``."""
         opts = opts or RunOptions()
         ms = C.c_double(0)
         arr = (_abi.Tallies * len(scenes))(*[_device_tallies(t) for t in tallies])
