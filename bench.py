@@ -339,7 +339,7 @@ def measure_batch(n_scenes: int, workdir: str, emissions_each: float = 1.0e8, re
                         "keV); scanner 32 rings, 128 rad x 128 ang x 1985 planes (span 1); device-resident tallies",
             "unit": UNIT, "tuned_batch_identical_to_tuned_sequential": identical,
             "sequential": {"ms": seq_ms, "wall_s": seq_wall, "value": rate(seq_c, seq_ms), "launches": n_scenes},
-            "batched": {"ms": bat_ms, "wall_s": bat_wall, "value": rate(bat_c, bat_ms), "launches": 1},
+            "batched": {"ms": bat_ms, "wall_s": bat_wall, "value": rate(bat_c, bat_ms), "calls": 1},
             "sequential_tuned": {"ms": seqt_ms, "wall_s": seqt_wall, "value": rate(seqt_c, seqt_ms),
                                  "launches": n_scenes},
             "autotune": tune,
@@ -470,7 +470,7 @@ def measure_beds(n_beds: int, workdir: str, emissions_total: float = 5.0e9) -> d
     return {"workload": f"body phantom 256x256x400 @ 2 mm, 10 tissues (lung 0.3, bone 1.85, hot organ 8x), "
                         f"{emissions_total:.0e} decays over {n_beds} bed positions 20 cm apart; scanner R=39 cm, "
                         f"256 rings x 4 mm, 384 x 384 x 12333 span-11 sinograms ({nbins} bins, int32) per bed",
-            "unit": UNIT, "batched": {"ms": bat_ms, "value": rate(bat_c, bat_ms), "launches": 1},
+            "unit": UNIT, "batched": {"ms": bat_ms, "value": rate(bat_c, bat_ms), "calls": 1},
             "one_by_one": {"ms": seq_ms, "value": rate(seq_c, seq_ms), "launches": n_beds},
             "coincidences_per_bed": per_bed, "highest_bin_bed0": top, "guard_trips": guard,
             "gradient_bed0": {"plain_forward_ms": plain, "forward_with_records_ms": r.forward_ms,
