@@ -31,12 +31,15 @@ struct LaneCounters {
 };
 
 /* Compile-time variants of the transport kernels (kMode bits): kModeFast
- * is the single-precision direction rotation, decay clock and photon-2
- * emission of balanced lanes; kModePrompt compiles the prompt-gamma emitter;
- * kModeCaps reads the loop guards' caps from the run parameters instead of
- * the defaults; kModeSino leaves out the phase-space (PSF) tally of runs that
- * tally the sinogram only.  A variant carries none of the code of the
- * features it leaves out. */
+ * is the arithmetic of balanced lanes (single-precision rotation, decay
+ * clock, photon-2 emission, Compton sampling, sinogram indices and energy
+ * blur; GCOa's normaliser from the interaction record's bound);
+ * kModePrompt compiles the prompt-gamma emitter; kModeCaps reads the loop
+ * guards' caps from the run parameters instead of the defaults; kModeSino
+ * leaves out the phase-space (PSF) tally of runs that tally the sinogram
+ * only; kModeChain makes the single-scene kernel a chained launch of a
+ * batched run (programmatic dependent launch, seed from the batch slot).  A
+ * variant carries none of the code of the features it leaves out. */
 constexpr int kModeFast = kTransportFast, kModePrompt = kTransportPrompt, kModeCaps = kTransportCaps,
               kModeSino = kTransportSinogramOnly, kModeChain = kTransportChained;
 
