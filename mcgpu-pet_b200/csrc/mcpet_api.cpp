@@ -427,10 +427,11 @@ mcpet_status ensure_device(mcpet_scene* sc) {
   return MCPET_OK;
 }
 
-/* Automatic decays per balanced lane: about 3 lanes per resident thread.
- * Fewer, longer lanes amortise the per-lane start (stream jump, emitter
- * search); on the 1e9-decay head workload the kernel time falls from 774 ms
- * at 16 lanes per thread to 748 ms at 3 and stays flat down to 1. */
+/* Automatic decays per balanced lane: about kAutoLanesPerThread (6) lanes
+ * per resident thread.  Fewer, longer lanes amortise the per-lane start
+ * (stream jump, emitter search), more lanes shorten the tail; on the
+ * 1e9-decay head workload: 399.2 ms at 1.5 lanes per thread, 384.2 ms at
+ * 3, 380.7 ms at 6, 382.5 ms at 12. */
 /* Sum of the emitting voxels' activity, cached until the activity changes. */
 double emitting_activity(const mcpet_scene* sc) {
   if (sc->emitting_activity < 0) {
@@ -446,7 +447,7 @@ int auto_hpl_of(const std::vector<const mcpet_scene*>& scenes) {
   double D = 0;
   for (const mcpet_scene* sc : scenes) D += emitting_activity(sc) * ((double)sc->cfg.acquisition_time_ps * 1e-12);
   double threads = (double)std::max(scenes[0]->dev.sm_count, 1) * 2048.0;
-  double h = D / (threads * 3.0);
+  double h = D / (threads * kAutoLanesPerThread);
   if (h < 1) h = 1;
   if (h > 4096) h = 4096;
   return (int)h;

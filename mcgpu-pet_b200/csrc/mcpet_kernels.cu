@@ -357,15 +357,15 @@ __global__ void plan_count_kernel(const float* act, int nvox, NoAllocScratch* S)
 }
 
 /* decays per balanced lane: the caller's value, or the automatic one from
- * the activity map on the device (expected decays over 3 lanes per
- * resident thread, clamped to [1, 4096]) */
+ * the activity map on the device (expected decays over kAutoLanesPerThread
+ * lanes per resident thread, clamped to [1, 4096], as on the host) */
 __global__ void plan_hpl_kernel(int n_chunks, double t_s, int hpl, double resident_threads, NoAllocScratch* S) {
   if (threadIdx.x != 0) return;
   unsigned long long h = (unsigned long long)(hpl > 0 ? hpl : 1);
   if (hpl <= 0) {
     double A = 0.0;
     for (int c = 0; c < n_chunks; ++c) A += S->chunk_activity[c];
-    double x = A * t_s / (resident_threads * 3.0);
+    double x = A * t_s / (resident_threads * kAutoLanesPerThread);
     if (x < 1) x = 1;
     if (x > 4096) x = 4096;
     h = (unsigned long long)(int)x;

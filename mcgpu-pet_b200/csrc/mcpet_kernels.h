@@ -21,6 +21,9 @@ constexpr int kTransportFast = 1;
 constexpr int kTransportPrompt = 2;
 constexpr int kTransportCaps = 4;
 constexpr int kTransportSinogramOnly = 8;   /* no PSF tally (and no sinogram-dry PSF replays) */
+/* automatic balanced lanes: expected decays spread over this many lanes per
+ * resident thread (host plans and device-built plans alike) */
+constexpr double kAutoLanesPerThread = 6.0;
 constexpr int kTransportChained = 16;       /* single-scene launch of a batched run that may follow another
                                                (programmatic dependent launch; seed read from the batch
                                                slot); plain event kernel, no loop caps */
